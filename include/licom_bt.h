@@ -1,0 +1,155 @@
+/*
+ * licom_bt.h - C-ABI of the B200 barotropic duogrid solver (libbt.so).
+ *
+ * The reference integrates the barotropic shallow-water equations with
+ * `_barotr_rk2_core(state, consts, nbb, dtb, px, py)` /
+ * `_barotr_rk3_core(...)` (src/licom/momentum/barotr.py:41-87), compiled once
+ * per run by `Schedule.configure` -> `make_spmd_jit`
+ * (src/licom/mymodule/schedule.py:209-243, src/licom/kernel/spmd.py:38-75)
+ * and called from `schedule_core` (schedule.py:148-190).  This library is the
+ * compiled form of that path on one GPU: a plan captures the 17 constants
+ * once (like the JIT's closure-captured consts) and every round advances a
+ * state by nbb substeps.
+ *
+ * Conventions
+ *   - Every field is a device array (6, M, M), M = N + 6, C order, in the
+ *     plan's dtype; matrices are (6, M, M, 2, 2), k2e_coef is (6, M, M, 2),
+ *     the k2e location tables are int32 (6, M, M).  Axis -2 is the Fortran i
+ *     index, axis -1 the Fortran j index.
+ *   - Calls are stream-ordered and non-blocking; pass a cudaStream_t as void*
+ *     (NULL = the legacy default stream).
+ *   - Every call returns BT_OK (0) or a negative code and never aborts; the
+ *     message is available from bt_last_error() (thread-local).
+ *   - A plan is not thread-safe: use one plan per host thread / stream.
+ */
+#ifndef LICOM_BT_H
+#define LICOM_BT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BT_OK 0
+#define BT_EINVAL -1   /* bad argument (shape, dtype, pointer, option) */
+#define BT_ENOMEM -2   /* device or host allocation failed */
+#define BT_ECUDA -3    /* a CUDA runtime call failed */
+#define BT_EDEVICE -4  /* a kernel reported an error through the plan's device flag */
+#define BT_ENOTSUP -5  /* valid input the solver does not support */
+
+#define BT_F64 0
+#define BT_F32 1
+
+/* Round execution modes */
+#define BT_MODE_STREAM 0      /* kernels launched in stream order */
+#define BT_MODE_GRAPH 1       /* the round is captured once as a CUDA graph and replayed */
+#define BT_MODE_PERSISTENT 2  /* one cooperative launch with grid barriers per round */
+
+typedef struct bt_plan bt_plan;
+
+/* Geometry of one resolution: the 17 constants in CONST_SOURCES order
+ * (src/licom/mymodule/schedule.py:95-116), as device pointers. */
+typedef struct bt_grid_desc {
+  int n;      /* cells per face edge N (>= 4) */
+  int dtype;  /* BT_F64 or BT_F32 */
+  const void* dzph_x;
+  const void* dzph_y;
+  const void* rdx;
+  const void* rdy;
+  const void* a_f;
+  const void* k2e_coef;
+  const int* loc_i_local;
+  const int* loc_j_local;
+  const void* a_c2l;
+  const void* a_l2c;
+  const void* inner;
+  const void* outer;
+  const void* a_gct;
+  const void* a_sina;
+  const void* rda;
+  const void* c_dy;
+  const void* d_dx;
+} bt_grid_desc;
+
+/* Round input: STATE_KEYS[0:6] = h0, h0p, ub, vb, ubp, vbp
+ * (src/licom/mymodule/schedule.py:62-92).  h0p/ubp/vbp may alias h0/ub/vb. */
+typedef struct bt_state_in {
+  const void* h0;
+  const void* h0p;
+  const void* ub;
+  const void* vb;
+  const void* ubp;
+  const void* vbp;
+} bt_state_in;
+
+/* Round output.  h0/ub/vb receive the new state (also the new h0p/ubp/vbp,
+ * barotr.py:59) with halos filled; they must not alias any input.  diag[0..9]
+ * receive STATE_KEYS[6:16] (celerity_x, celerity_y, ub_ct, vb_ct, ub_cx,
+ * ub_cy, vb_cx, vb_cy, advx, advy) of the last stage; pass NULL in diag[0]
+ * to skip the diagnostics. */
+typedef struct bt_state_out {
+  void* h0;
+  void* ub;
+  void* vb;
+  void* diag[10];
+} bt_state_out;
+
+/* Build a plan: validates the masks, builds the halo gather tables from
+ * k2e_coef/loc_i/loc_j and the cube topology, allocates the stage scratch.
+ * Replaces Schedule.configure/make_spmd_jit (schedule.py:209-243, spmd.py:38-75)
+ * and Communication.configure (src/licom/kernel/communication.py:269-291).
+ * The constant arrays must stay alive and unchanged while the plan exists. */
+int bt_plan_create(const bt_grid_desc* desc, bt_plan** out);
+
+/* Release a plan and everything it owns (no counterpart: JAX frees by refcount). */
+int bt_plan_destroy(bt_plan* plan);
+
+/* Tile shape (rows ti x columns tj of interior cells per CTA) and round mode. */
+int bt_plan_set_tile(bt_plan* plan, int ti, int tj);
+int bt_plan_set_mode(bt_plan* plan, int mode);
+
+/* Advance nbb (>= 1) substeps of RK2 (rk = 2, midpoint, barotr.py:41-61) or
+ * RK3 (rk = 3, barotr.py:64-87) with step dtb.  Replaces the call
+ * rk_core(barotr_s, barotr_consts, nbb, dtb, px, py) (schedule.py:170) with
+ * px = py = 1; STATE_KEYS[16:23] pass through untouched and are not handled here. */
+int bt_round(bt_plan* plan, const bt_state_in* in, const bt_state_out* out, int nbb, double dtb,
+             int rk, void* stream);
+
+/* One RK stage: _step_rk_logic(h0, h0p, ub, vb, ubp, vbp, consts, dt, beta_d,
+ * is_laststep, px, py) (src/licom/momentum/barotr_pure.py:100-168).  The
+ * inputs' halo cells are used as given; out->h0/ub/vb receive new_h0/new_ub/
+ * new_vb with filled halos, out->diag[0..9] the ten diagnostics of the stage
+ * (computed from its inputs), or pass diag[0] = NULL to skip them. */
+int bt_stage(bt_plan* plan, const bt_state_in* in, const bt_state_out* out, double dt, double beta_d,
+             int is_laststep, void* stream);
+
+/* Fill the halo cells of a scalar field h and/or a vector (u, v) from their
+ * interiors: ext_scalar / ext_vector (src/licom/kernel/cube.py:130-153).
+ * Any of h, u (with v) may be NULL. */
+int bt_fill_halo(bt_plan* plan, void* h, void* u, void* v, void* stream);
+
+/* Edge average of the face-normal C-grid components of (u, v) in place:
+ * Communication.boundary_communication (communication.py:504-570). */
+int bt_edge_average(bt_plan* plan, void* u, void* v, void* stream);
+
+/* Host-only: the halo gather tables a plan builds, for inspection and testing.
+ * For n cells per face edge (M = n + 6, nh = 12 n + 36 halo cells per face):
+ * src (6*nh*2 int32, absolute source cell offsets within a (6,M,M) field),
+ * weights (6*nh*2), route (24 packed entries nb | side << 4 | rev << 6).
+ * Halo cell (i, j) of face f has index f*nh + id, id numbering rows 0..2,
+ * rows M-3..M-1 (all columns), then the W and E bands row by row.  Together
+ * with the c2l/l2c rotations these tables reproduce ext_scalar/ext_vector
+ * (cube.py:40-153) and the halo routing of communication.py:269-474. */
+int bt_halo_table_host(int n, const double* k2e_coef, const int* loc_i, const int* loc_j, int* src,
+                       double* weights, int* route);
+
+/* Synchronise the plan's work and report a device-side error flag, if set. */
+int bt_check_device_error(bt_plan* plan);
+
+const char* bt_last_error(void);
+int bt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LICOM_BT_H */

@@ -29,7 +29,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CXX = os.environ.get("CXX", shutil.which("g++") or "g++")
 
 CUDA_SOURCES = ["bt_kernels.cu", "bt_capi.cu"]
-CUDA_HEADERS = ["bt_common.cuh", "bt_stencil.cuh"]
+CUDA_HEADERS = ["bt_common.cuh", "bt_stencil.cuh", "bt_launch.cuh"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -67,7 +67,9 @@ def build_bt(force: bool = False, verbose_ptxas: bool = False) -> str:
     deps = srcs + [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [
         os.path.join(INCLUDE, "licom_bt.h"), __file__]
     if force or _newer(out, deps):
-        cmd = [NVCC, *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "--shared",
+        # -fmad=false: no FMA contraction, so the float64 kernels round like the
+        # reference's float64 NumPy/XLA arithmetic term by term.
+        cmd = [NVCC, *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "-fmad=false", "--shared",
                "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC, "-lcudart",
                *srcs, "-o", out + ".tmp"]
         if verbose_ptxas:

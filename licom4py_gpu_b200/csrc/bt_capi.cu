@@ -1,0 +1,561 @@
+// bt_capi.cu - plan construction and the C-ABI of libbt.so (see include/licom_bt.h).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bt_launch.cuh"
+#include "licom_bt.h"
+
+using namespace bt;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(BT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define BT_CUDA(call, what)                  \
+  do {                                       \
+    cudaError_t e_ = (call);                 \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+// Cube adjacency for side d of face t (0-based faces, sides E W N S = 0..3):
+// even/odd face rules of the reference topology (communication.py:57-87); the
+// along-edge index is reversed when an E/W side meets an S/N side
+// (communication.py:41-55).
+void face_neighbor(int t, int d, int* nb, int* side, int* rev) {
+  if (t % 2 == 0) {
+    switch (d) {
+      case kS: *nb = (t + 4) % 6; *side = kE; break;
+      case kE: *nb = (t + 2) % 6; *side = kS; break;
+      case kN: *nb = (t + 1) % 6; *side = kS; break;
+      default: *nb = (t + 5) % 6; *side = kE; break;
+    }
+  } else {
+    switch (d) {
+      case kE: *nb = (t + 1) % 6; *side = kW; break;
+      case kN: *nb = (t + 2) % 6; *side = kW; break;
+      case kW: *nb = (t + 4) % 6; *side = kN; break;
+      default: *nb = (t + 5) % 6; *side = kN; break;
+    }
+  }
+  const bool ew_a = (d == kE || d == kW), ew_b = (*side == kE || *side == kW);
+  *rev = (ew_a != ew_b) ? 1 : 0;
+}
+
+// Interior cell on line c (0..2, in the order of communication.py:193-207)
+// and along-edge position k next to ``side``.
+void side_line_cell(int side, int c, int k, int m, int* i, int* j) {
+  switch (side) {
+    case kE: *i = kHalo + k; *j = m - 6 + c; break;
+    case kW: *i = kHalo + k; *j = kHalo + c; break;
+    case kN: *i = m - 6 + c; *j = kHalo + k; break;
+    default: *i = kHalo + c; *j = kHalo + k; break;
+  }
+}
+
+// Halo cell written from line c at position k of the band on side d
+// (communication.py:210-223 without corners).
+void band_cell(int d, int c, int k, int m, int* i, int* j) {
+  switch (d) {
+    case kE: *i = kHalo + k; *j = m - kHalo + c; break;
+    case kW: *i = kHalo + k; *j = c; break;
+    case kN: *i = m - kHalo + c; *j = kHalo + k; break;
+    default: *i = c; *j = kHalo + k; break;
+  }
+}
+
+}  // namespace
+
+struct bt_plan {
+  int n = 0, m = 0, nh = 0, dtype = BT_F64, device = 0;
+  TileCfg tile{8, 32};
+  int mode = BT_MODE_STREAM;
+  const void* c[17] = {};
+  int route[24] = {};
+  void* d_hsrc = nullptr;  // int2[6*nh]
+  void* d_hw = nullptr;    // T[6*nh*2]
+  void* scratch = nullptr; // Y (3 fields) + Y2 (3 fields) + edge lines
+  size_t field_elems = 0;
+  cudaStream_t cap_stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // graph cache
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<uintptr_t> gkey;
+
+  size_t esize() const { return dtype == BT_F64 ? 8 : 4; }
+  void* scratch_field(int k) const { return (char*)scratch + (size_t)k * field_elems * esize(); }
+  void* edge_lines() const { return scratch_field(6); }
+
+  template <typename T>
+  Geo<T> geo() const {
+    Geo<T> g;
+    g.n = n;
+    g.m = m;
+    g.nh = nh;
+    g.dzph_x = (const T*)c[0];
+    g.dzph_y = (const T*)c[1];
+    g.rdx = (const T*)c[2];
+    g.rdy = (const T*)c[3];
+    g.a_f = (const T*)c[4];
+    g.c2l = (const T*)c[8];
+    g.l2c = (const T*)c[9];
+    g.gct = (const T*)c[12];
+    g.sina = (const T*)c[13];
+    g.rda = (const T*)c[14];
+    g.c_dy = (const T*)c[15];
+    g.d_dx = (const T*)c[16];
+    g.hsrc = (const int2*)d_hsrc;
+    g.hw = (const T*)d_hw;
+    std::memcpy(g.route, route, sizeof(route));
+    return g;
+  }
+};
+
+namespace {
+
+// Halo gather tables of one resolution, host side: for every halo cell of
+// every face, the two neighbour-interior source cells and the two linear
+// interpolation weights (composition of communication.py:387-474 and
+// cube.py:40-127); route[f*4+side] packs the adjacency.
+template <typename T>
+int build_halo_host(int n, const T* coef, const int* li, const int* lj, int2* src, T* w, int* route) {
+  const int m = n + 6, nh = halo_count(m);
+  const size_t fe = (size_t)6 * m * m;
+  for (int f = 0; f < 6; ++f)
+    for (int dd = 0; dd < 4; ++dd) {
+      int nb, side, rev;
+      face_neighbor(f, dd, &nb, &side, &rev);
+      route[f * 4 + dd] = route_pack(nb, side, rev);
+    }
+  // halo copy map: halo band cell -> neighbour interior cell
+  std::vector<long> copy(fe, -1);
+  for (int f = 0; f < 6; ++f)
+    for (int dd = 0; dd < 4; ++dd) {
+      int nb, side, rev;
+      face_neighbor(f, dd, &nb, &side, &rev);
+      for (int c = 0; c < kHalo; ++c)
+        for (int k = 0; k < n; ++k) {
+          const int kk = rev ? n - 1 - k : k;
+          int si, sj, ti, tj;
+          side_line_cell(side, c, kk, m, &si, &sj);
+          band_cell(dd, c, k, m, &ti, &tj);
+          copy[cell(f, ti, tj, m)] = cell(nb, si, sj, m);
+        }
+    }
+  // kinked->extended interpolation along the band; corners copy the band cell
+  // of row 3 / M-4 (cube.py:64-125)
+  for (int f = 0; f < 6; ++f)
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) {
+        if (is_interior(i, j, m)) continue;
+        int bi = i;
+        const int bj = j;
+        const bool corner = (i < kHalo || i >= m - kHalo) && (j < kHalo || j >= m - kHalo);
+        if (corner) bi = (i < kHalo) ? kHalo : m - kHalo - 1;
+        const long ob = cell(f, bi, bj, m);
+        const bool along_i = (bj < kHalo || bj >= m - kHalo);  // W/E band: interpolate along axis -2
+        const int loc = along_i ? li[ob] : lj[ob];
+        if (loc < kHalo || loc > m - kHalo - 2)
+          return fail(BT_EINVAL, "k2e location table out of range at a halo cell (face " + std::to_string(f) +
+                                     ", " + std::to_string(bi) + ", " + std::to_string(bj) + ")");
+        long s0, s1;
+        if (along_i) {
+          s0 = copy[cell(f, loc, bj, m)];
+          s1 = copy[cell(f, loc + 1, bj, m)];
+        } else {
+          s0 = copy[cell(f, bi, loc, m)];
+          s1 = copy[cell(f, bi, loc + 1, m)];
+        }
+        if (s0 < 0 || s1 < 0) return fail(BT_EINVAL, "halo gather source is not a band cell");
+        const size_t k = (size_t)f * nh + halo_id(i, j, m);
+        src[k] = make_int2((int)s0, (int)s1);
+        w[2 * k] = coef[2 * ob];
+        w[2 * k + 1] = coef[2 * ob + 1];
+      }
+  return BT_OK;
+}
+
+template <typename T>
+int build_tables(bt_plan* p, const bt_grid_desc* d) {
+  const int m = p->m, nh = p->nh;
+  const size_t fe = (size_t)6 * m * m;
+  std::vector<T> coef(fe * 2), inner(fe), outer(fe);
+  std::vector<int> li(fe), lj(fe);
+  BT_CUDA(cudaMemcpy(coef.data(), d->k2e_coef, coef.size() * sizeof(T), cudaMemcpyDeviceToHost), "copy k2e_coef");
+  BT_CUDA(cudaMemcpy(li.data(), d->loc_i_local, li.size() * sizeof(int), cudaMemcpyDeviceToHost), "copy loc_i");
+  BT_CUDA(cudaMemcpy(lj.data(), d->loc_j_local, lj.size() * sizeof(int), cudaMemcpyDeviceToHost), "copy loc_j");
+  BT_CUDA(cudaMemcpy(inner.data(), d->inner, fe * sizeof(T), cudaMemcpyDeviceToHost), "copy inner");
+  BT_CUDA(cudaMemcpy(outer.data(), d->outer, fe * sizeof(T), cudaMemcpyDeviceToHost), "copy outer");
+  // The kernels apply the ext_vector masks as exact 1/0 (cube.py:139-151): check them.
+  for (int f = 0; f < 6; ++f)
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) {
+        const long o = cell(f, i, j, m);
+        const T want = is_interior(i, j, m) ? T(1) : T(0);
+        if (inner[o] != want || outer[o] != T(1) - want)
+          return fail(BT_ENOTSUP, "inner/outer must be the interior/halo masks of duogrid.py:159-190");
+      }
+  std::vector<int2> src((size_t)6 * nh);
+  std::vector<T> w((size_t)6 * nh * 2);
+  const int rc = build_halo_host<T>(p->n, coef.data(), li.data(), lj.data(), src.data(), w.data(), p->route);
+  if (rc != BT_OK) return rc;
+  BT_CUDA(cudaMalloc(&p->d_hsrc, src.size() * sizeof(int2)), "alloc halo table");
+  BT_CUDA(cudaMalloc(&p->d_hw, w.size() * sizeof(T)), "alloc halo weights");
+  BT_CUDA(cudaMemcpy(p->d_hsrc, src.data(), src.size() * sizeof(int2), cudaMemcpyHostToDevice), "upload table");
+  BT_CUDA(cudaMemcpy(p->d_hw, w.data(), w.size() * sizeof(T), cudaMemcpyHostToDevice), "upload weights");
+  return BT_OK;
+}
+
+template <typename T>
+StageIO<T> stage_io(const T* h, const T* u, const T* v, const T* hp, const T* up, const T* vp, T* ho, T* uo,
+                    T* vo, double dt, double beta, int stored, int last) {
+  StageIO<T> io;
+  io.h = h;
+  io.u = u;
+  io.v = v;
+  io.hp = hp;
+  io.up = up;
+  io.vp = vp;
+  io.h_out = ho;
+  io.u_out = uo;
+  io.v_out = vo;
+  io.dt = (T)dt;
+  io.beta = (T)beta;
+  io.stored_halo = stored;
+  io.last = last;
+  return io;
+}
+
+template <typename T>
+cudaError_t run_stage(const bt_plan* p, const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
+  cudaError_t e = launch_phase_h<T>(g, io, p->tile, s);
+  if (e != cudaSuccess) return e;
+  return launch_phase_uv<T>(g, io, p->tile, s);
+}
+
+// The launch sequence of one round (stream order).
+template <typename T>
+cudaError_t enqueue_round(const bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb,
+                          double dtb, int rk, cudaStream_t s) {
+  const Geo<T> g = p->geo<T>();
+  T* Y[3] = {(T*)p->scratch_field(0), (T*)p->scratch_field(1), (T*)p->scratch_field(2)};
+  T* Z[3] = {(T*)p->scratch_field(3), (T*)p->scratch_field(4), (T*)p->scratch_field(5)};
+  T* X[3] = {(T*)out.h0, (T*)out.ub, (T*)out.vb};
+  const T* X0[3] = {(const T*)in.h0, (const T*)in.ub, (const T*)in.vb};
+  const T* B0[3] = {(const T*)in.h0p, (const T*)in.ubp, (const T*)in.vbp};
+  cudaError_t e = cudaSuccess;
+  for (int step = 0; step < nbb; ++step) {
+    const T* const* cur = step == 0 ? X0 : (const T* const*)X;
+    const T* const* base = step == 0 ? B0 : (const T* const*)X;
+    const int stored = step == 0 ? 1 : 0;
+    if (rk == 2) {
+      // barotr.py:50-56: dt/2 from the base, then dt from the same base
+      e = run_stage<T>(p, g, stage_io<T>(cur[0], cur[1], cur[2], base[0], base[1], base[2], Y[0], Y[1], Y[2],
+                                         dtb / 2.0, 0.0, stored, 0), s);
+      if (e != cudaSuccess) return e;
+      e = run_stage<T>(p, g, stage_io<T>(Y[0], Y[1], Y[2], base[0], base[1], base[2], X[0], X[1], X[2], dtb,
+                                         0.0, 0, 1), s);
+    } else {
+      // barotr.py:73-83: dt/3, dt/2, dt with beta_d = 1
+      e = run_stage<T>(p, g, stage_io<T>(cur[0], cur[1], cur[2], base[0], base[1], base[2], Y[0], Y[1], Y[2],
+                                         dtb / 3.0, 1.0, stored, 0), s);
+      if (e != cudaSuccess) return e;
+      e = run_stage<T>(p, g, stage_io<T>(Y[0], Y[1], Y[2], base[0], base[1], base[2], Z[0], Z[1], Z[2],
+                                         dtb / 2.0, 1.0, 0, 0), s);
+      if (e != cudaSuccess) return e;
+      e = run_stage<T>(p, g, stage_io<T>(Z[0], Z[1], Z[2], base[0], base[1], base[2], X[0], X[1], X[2], dtb,
+                                         1.0, 0, 1), s);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  if (out.diag[0]) {
+    T* const* L = rk == 2 ? Y : Z;  // input of the last stage
+    e = launch_fill_halo<T>(g, L[0], L[1], L[2], s);
+    if (e != cudaSuccess) return e;
+    DiagOut<T> d;
+    T** dp = (T**)&d;
+    for (int k = 0; k < 10; ++k) dp[k] = (T*)out.diag[k];
+    e = launch_diag<T>(g, L[0], L[1], L[2], d, s);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_fill_halo<T>(g, X[0], X[1], X[2], s);
+}
+
+template <typename T>
+cudaError_t enqueue_stage(const bt_plan* p, const bt_state_in& in, const bt_state_out& out, double dt,
+                          double beta, int last, cudaStream_t s) {
+  const Geo<T> g = p->geo<T>();
+  T* X[3] = {(T*)out.h0, (T*)out.ub, (T*)out.vb};
+  const StageIO<T> io = stage_io<T>((const T*)in.h0, (const T*)in.ub, (const T*)in.vb, (const T*)in.h0p,
+                                    (const T*)in.ubp, (const T*)in.vbp, X[0], X[1], X[2], dt, beta, 1, last);
+  cudaError_t e = run_stage<T>(p, g, io, s);
+  if (e != cudaSuccess) return e;
+  if (out.diag[0]) {
+    DiagOut<T> d;
+    T** dp = (T**)&d;
+    for (int k = 0; k < 10; ++k) dp[k] = (T*)out.diag[k];
+    e = launch_diag<T>(g, (const T*)in.h0, (const T*)in.ub, (const T*)in.vb, d, s);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_fill_halo<T>(g, X[0], X[1], X[2], s);
+}
+
+cudaError_t enqueue(const bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb, double dtb,
+                    int rk, cudaStream_t s) {
+  return p->dtype == BT_F64 ? enqueue_round<double>(p, in, out, nbb, dtb, rk, s)
+                            : enqueue_round<float>(p, in, out, nbb, dtb, rk, s);
+}
+
+// ---- edge average kernels (bt_edge_average) --------------------------------
+template <typename T>
+__global__ void k_edge_gather(Geo<T> g, const T* u, const T* v, T* lines) {
+  const int n = g.n, m = g.m;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 24 * n) return;
+  const int fd = k / n, q = k - fd * n, f = fd / 4, d = fd % 4;
+  long o;
+  const T* src;
+  switch (d) {
+    case kE: o = cell(f, kHalo + q, m - kHalo, m); src = v; break;
+    case kW: o = cell(f, kHalo + q, kHalo, m); src = v; break;
+    case kN: o = cell(f, m - kHalo, kHalo + q, m); src = u; break;
+    default: o = cell(f, kHalo, kHalo + q, m); src = u; break;
+  }
+  lines[k] = src[o];
+}
+
+template <typename T>
+__global__ void k_edge_apply(Geo<T> g, T* u, T* v, const T* lines) {
+  const int n = g.n, m = g.m;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 24 * n) return;
+  const int fd = k / n, q = k - fd * n, f = fd / 4, d = fd % 4;
+  const int r = g.route[fd];
+  const int kk = route_rev(r) ? n - 1 - q : q;
+  const T val = (lines[k] + lines[(route_nb(r) * 4 + route_side(r)) * n + kk]) / T(2.0);
+  switch (d) {
+    case kE: v[cell(f, kHalo + q, m - kHalo, m)] = val; break;
+    case kW: v[cell(f, kHalo + q, kHalo, m)] = val; break;
+    case kN: u[cell(f, m - kHalo, kHalo + q, m)] = val; break;
+    default: u[cell(f, kHalo, kHalo + q, m)] = val; break;
+  }
+}
+
+template <typename T>
+cudaError_t enqueue_edge_average(const bt_plan* p, void* u, void* v, cudaStream_t s) {
+  const Geo<T> g = p->geo<T>();
+  const int total = 24 * p->n, th = 128, bl = (total + th - 1) / th;
+  k_edge_gather<T><<<bl, th, 0, s>>>(g, (const T*)u, (const T*)v, (T*)p->edge_lines());
+  k_edge_apply<T><<<bl, th, 0, s>>>(g, (T*)u, (T*)v, (const T*)p->edge_lines());
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+int bt_version(void) { return 1; }
+
+int bt_halo_table_host(int n, const double* k2e_coef, const int* loc_i, const int* loc_j, int* src,
+                       double* weights, int* route) {
+  if (n < 4 || !k2e_coef || !loc_i || !loc_j || !src || !weights || !route)
+    return fail(BT_EINVAL, "bt_halo_table_host: bad argument");
+  return build_halo_host<double>(n, k2e_coef, loc_i, loc_j, (int2*)src, weights, route);
+}
+
+const char* bt_last_error(void) { return g_err.c_str(); }
+
+int bt_plan_create(const bt_grid_desc* d, bt_plan** out) {
+  if (!d || !out) return fail(BT_EINVAL, "bt_plan_create: NULL argument");
+  *out = nullptr;
+  if (d->n < 4 || d->n > 8192) return fail(BT_EINVAL, "bt_plan_create: n must be in [4, 8192]");
+  if (d->dtype != BT_F64 && d->dtype != BT_F32) return fail(BT_EINVAL, "bt_plan_create: dtype must be BT_F64 or BT_F32");
+  const void* cs[17] = {d->dzph_x, d->dzph_y, d->rdx, d->rdy, d->a_f, d->k2e_coef, d->loc_i_local,
+                        d->loc_j_local, d->a_c2l, d->a_l2c, d->inner, d->outer, d->a_gct, d->a_sina,
+                        d->rda, d->c_dy, d->d_dx};
+  for (int k = 0; k < 17; ++k)
+    if (!cs[k]) return fail(BT_EINVAL, "bt_plan_create: constant pointer " + std::to_string(k) + " is NULL");
+  bt_plan* p = new bt_plan;
+  p->n = d->n;
+  p->m = d->n + 6;
+  p->nh = halo_count(p->m);
+  p->dtype = d->dtype;
+  std::memcpy(p->c, cs, sizeof(cs));
+  cudaGetDevice(&p->device);
+  p->field_elems = (size_t)6 * p->m * p->m;
+  cudaError_t pe = p->dtype == BT_F64 ? prime_kernels<double>() : prime_kernels<float>();
+  if (pe != cudaSuccess) {
+    bt_plan_destroy(p);
+    return cuda_fail(pe, "bt_plan_create: kernel attributes");
+  }
+  int rc = p->dtype == BT_F64 ? build_tables<double>(p, d) : build_tables<float>(p, d);
+  if (rc != BT_OK) {
+    bt_plan_destroy(p);
+    return rc;
+  }
+  const size_t bytes = (6 * p->field_elems + 24 * (size_t)p->n) * p->esize();
+  cudaError_t e = cudaMalloc(&p->scratch, bytes);
+  if (e != cudaSuccess) {
+    bt_plan_destroy(p);
+    return fail(BT_ENOMEM, std::string("bt_plan_create: scratch allocation: ") + cudaGetErrorString(e));
+  }
+  e = cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    bt_plan_destroy(p);
+    return cuda_fail(e, "bt_plan_create: stream/event");
+  }
+  *out = p;
+  return BT_OK;
+}
+
+int bt_plan_destroy(bt_plan* p) {
+  if (!p) return BT_OK;
+  if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  if (p->ev_in) cudaEventDestroy(p->ev_in);
+  if (p->ev_out) cudaEventDestroy(p->ev_out);
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  if (p->scratch) cudaFree(p->scratch);
+  if (p->d_hsrc) cudaFree(p->d_hsrc);
+  if (p->d_hw) cudaFree(p->d_hw);
+  delete p;
+  return BT_OK;
+}
+
+int bt_plan_set_tile(bt_plan* p, int ti, int tj) {
+  if (!p) return fail(BT_EINVAL, "bt_plan_set_tile: NULL plan");
+  if (!tile_cfg_supported({ti, tj})) return fail(BT_EINVAL, "bt_plan_set_tile: unsupported tile shape");
+  p->tile = {ti, tj};
+  if (p->gexec) {
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+    p->gkey.clear();
+  }
+  return BT_OK;
+}
+
+int bt_plan_set_mode(bt_plan* p, int mode) {
+  if (!p) return fail(BT_EINVAL, "bt_plan_set_mode: NULL plan");
+  if (mode != BT_MODE_STREAM && mode != BT_MODE_GRAPH)
+    return fail(BT_ENOTSUP, "bt_plan_set_mode: mode not available in this build");
+  p->mode = mode;
+  return BT_OK;
+}
+
+int bt_round(bt_plan* p, const bt_state_in* in, const bt_state_out* out, int nbb, double dtb, int rk,
+             void* stream) {
+  if (!p || !in || !out) return fail(BT_EINVAL, "bt_round: NULL argument");
+  if (rk != 2 && rk != 3) return fail(BT_EINVAL, "bt_round: rk must be 2 or 3");
+  if (nbb < 1) return fail(BT_EINVAL, "bt_round: nbb must be >= 1");
+  const void* ins[6] = {in->h0, in->h0p, in->ub, in->vb, in->ubp, in->vbp};
+  for (const void* q : ins)
+    if (!q) return fail(BT_EINVAL, "bt_round: NULL input field");
+  if (!out->h0 || !out->ub || !out->vb) return fail(BT_EINVAL, "bt_round: NULL output field");
+  for (const void* q : ins)
+    if (q == out->h0 || q == out->ub || q == out->vb)
+      return fail(BT_EINVAL, "bt_round: output fields must not alias the inputs");
+  if (out->diag[0])
+    for (int k = 1; k < 10; ++k)
+      if (!out->diag[k]) return fail(BT_EINVAL, "bt_round: diag outputs must be all set or diag[0] NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->mode == BT_MODE_STREAM) {
+    cudaError_t e = enqueue(p, *in, *out, nbb, dtb, rk, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bt_round: launch");
+    return BT_OK;
+  }
+  // graph mode: capture once per (nbb, rk, dtb, pointers), replay afterwards
+  std::vector<uintptr_t> key = {(uintptr_t)nbb, (uintptr_t)rk};
+  uint64_t dbits;
+  std::memcpy(&dbits, &dtb, 8);
+  key.push_back((uintptr_t)dbits);
+  for (const void* q : ins) key.push_back((uintptr_t)q);
+  key.push_back((uintptr_t)out->h0);
+  key.push_back((uintptr_t)out->ub);
+  key.push_back((uintptr_t)out->vb);
+  for (int k = 0; k < 10; ++k) key.push_back((uintptr_t)out->diag[k]);
+  BT_CUDA(cudaEventRecord(p->ev_in, s), "bt_round: event record");
+  BT_CUDA(cudaStreamWaitEvent(p->cap_stream, p->ev_in, 0), "bt_round: stream wait");
+  if (!p->gexec || key != p->gkey) {
+    if (p->gexec) {
+      cudaGraphExecDestroy(p->gexec);
+      p->gexec = nullptr;
+    }
+    cudaGraph_t graph;
+    BT_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal), "bt_round: begin capture");
+    cudaError_t e = enqueue(p, *in, *out, nbb, dtb, rk, p->cap_stream);
+    cudaError_t e2 = cudaStreamEndCapture(p->cap_stream, &graph);
+    if (e != cudaSuccess) return cuda_fail(e, "bt_round: capture launch");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "bt_round: end capture");
+    e = cudaGraphInstantiate(&p->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "bt_round: graph instantiate");
+    p->gkey = key;
+  }
+  BT_CUDA(cudaGraphLaunch(p->gexec, p->cap_stream), "bt_round: graph launch");
+  BT_CUDA(cudaEventRecord(p->ev_out, p->cap_stream), "bt_round: event record");
+  BT_CUDA(cudaStreamWaitEvent(s, p->ev_out, 0), "bt_round: stream wait");
+  return BT_OK;
+}
+
+int bt_stage(bt_plan* p, const bt_state_in* in, const bt_state_out* out, double dt, double beta_d,
+             int is_laststep, void* stream) {
+  if (!p || !in || !out) return fail(BT_EINVAL, "bt_stage: NULL argument");
+  const void* ins[6] = {in->h0, in->h0p, in->ub, in->vb, in->ubp, in->vbp};
+  for (const void* q : ins)
+    if (!q) return fail(BT_EINVAL, "bt_stage: NULL input field");
+  if (!out->h0 || !out->ub || !out->vb) return fail(BT_EINVAL, "bt_stage: NULL output field");
+  for (const void* q : ins)
+    if (q == out->h0 || q == out->ub || q == out->vb)
+      return fail(BT_EINVAL, "bt_stage: output fields must not alias the inputs");
+  if (out->diag[0])
+    for (int k = 1; k < 10; ++k)
+      if (!out->diag[k]) return fail(BT_EINVAL, "bt_stage: diag outputs must be all set or diag[0] NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = p->dtype == BT_F64 ? enqueue_stage<double>(p, *in, *out, dt, beta_d, is_laststep ? 1 : 0, s)
+                                     : enqueue_stage<float>(p, *in, *out, dt, beta_d, is_laststep ? 1 : 0, s);
+  if (e != cudaSuccess) return cuda_fail(e, "bt_stage: launch");
+  return BT_OK;
+}
+
+int bt_fill_halo(bt_plan* p, void* h, void* u, void* v, void* stream) {
+  if (!p) return fail(BT_EINVAL, "bt_fill_halo: NULL plan");
+  if ((u == nullptr) != (v == nullptr)) return fail(BT_EINVAL, "bt_fill_halo: u and v must both be set or NULL");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = p->dtype == BT_F64
+                      ? launch_fill_halo<double>(p->geo<double>(), (double*)h, (double*)u, (double*)v, s)
+                      : launch_fill_halo<float>(p->geo<float>(), (float*)h, (float*)u, (float*)v, s);
+  if (e != cudaSuccess) return cuda_fail(e, "bt_fill_halo");
+  return BT_OK;
+}
+
+int bt_edge_average(bt_plan* p, void* u, void* v, void* stream) {
+  if (!p || !u || !v) return fail(BT_EINVAL, "bt_edge_average: NULL argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = p->dtype == BT_F64 ? enqueue_edge_average<double>(p, u, v, s)
+                                     : enqueue_edge_average<float>(p, u, v, s);
+  if (e != cudaSuccess) return cuda_fail(e, "bt_edge_average");
+  return BT_OK;
+}
+
+int bt_check_device_error(bt_plan* p) {
+  if (!p) return fail(BT_EINVAL, "bt_check_device_error: NULL plan");
+  BT_CUDA(cudaDeviceSynchronize(), "bt_check_device_error: synchronize");
+  return BT_OK;
+}
+
+}  // extern "C"

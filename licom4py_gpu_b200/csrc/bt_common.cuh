@@ -1,0 +1,102 @@
+// bt_common.cuh - shared types of the barotropic duogrid solver (device + host).
+//
+// One "member" is one barotropic integration: six cubed-sphere faces of
+// N x N cells, stored like the reference as (6, M, M) arrays, M = N + 6
+// (3-cell halo per side), row-major, axis -2 = Fortran i ("x"), axis -1 =
+// Fortran j ("y").  All six faces of a member live on one GPU.
+//
+// Halo cells are never exchanged between devices.  During a round they are
+// not materialised at all: a kernel that needs a halo value computes it from
+// the neighbouring face's interior through a precomputed gather table
+// (two source cells and two linear-interpolation weights per halo cell, the
+// composition of the reference's halo copy and kinked->extended remap), and
+// for vectors through the c2l/l2c rotations.  Halos are written out only at
+// the end of a round, for the returned state.
+
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bt {
+
+constexpr int kHalo = 3;
+enum Side { kE = 0, kW = 1, kN = 2, kS = 3 };  // communication.py:32
+
+// Linear offset of cell (i, j) of face f in a member's (6, M, M) field.
+__host__ __device__ __forceinline__ long cell(int f, int i, int j, int m) {
+  return ((long)f * m + i) * m + j;
+}
+
+// Number of halo cells per face and the id of halo cell (i, j) in [0, nh).
+// Order: rows 0..2 (all columns), rows M-3..M-1 (all columns), then the W
+// band (rows 3..M-4, cols 0..2) and the E band (rows 3..M-4, cols M-3..M-1).
+__host__ __device__ __forceinline__ int halo_count(int m) { return 12 * (m - 6) + 36; }
+
+__host__ __device__ __forceinline__ bool is_interior(int i, int j, int m) {
+  return i >= kHalo && i < m - kHalo && j >= kHalo && j < m - kHalo;
+}
+
+__host__ __device__ __forceinline__ int halo_id(int i, int j, int m) {
+  if (i < kHalo) return i * m + j;
+  if (i >= m - kHalo) return 3 * m + (i - (m - kHalo)) * m + j;
+  const int n = m - 6;
+  if (j < kHalo) return 6 * m + (i - kHalo) * 3 + j;
+  return 6 * m + 3 * n + (i - kHalo) * 3 + (j - (m - kHalo));
+}
+
+// Routing entry for side d of face f: neighbour face, its side, reversed flag.
+__host__ __device__ __forceinline__ int route_pack(int nb, int side, int rev) {
+  return nb | (side << 4) | (rev << 6);
+}
+__host__ __device__ __forceinline__ int route_nb(int r) { return r & 15; }
+__host__ __device__ __forceinline__ int route_side(int r) { return (r >> 4) & 3; }
+__host__ __device__ __forceinline__ int route_rev(int r) { return (r >> 6) & 1; }
+
+// Geometry of one resolution (shared by every member of that resolution).
+template <typename T>
+struct Geo {
+  int n, m, nh;
+  const T* dzph_x;  // (6,M,M)
+  const T* dzph_y;
+  const T* rdx;
+  const T* rdy;
+  const T* a_f;
+  const T* c2l;     // (6,M,M,2,2)
+  const T* l2c;     // (6,M,M,2,2)
+  const T* gct;     // (6,M,M,2,2)
+  const T* sina;
+  const T* rda;
+  const T* c_dy;
+  const T* d_dx;
+  const int2* hsrc; // (6, nh) source offsets (absolute within the member)
+  const T* hw;      // (6, nh, 2) interpolation weights
+  int route[24];    // f*4 + side
+};
+
+// Pointers of one RK stage of one member.
+template <typename T>
+struct StageIO {
+  const T* h;   // stage input (stencil reads)
+  const T* u;
+  const T* v;
+  const T* hp;  // RK base (pointwise reads)
+  const T* up;
+  const T* vp;
+  T* h_out;     // stage outputs (interior cells only)
+  T* u_out;
+  T* v_out;
+  T dt;
+  T beta;
+  int stored_halo;  // 1: the inputs' halo cells hold valid values (first stage of a round)
+  int last;         // 1: last stage of the substep (mass-flux edge average active)
+};
+
+// Tile decomposition of the N x N interior of each face.
+struct Tiling {
+  int ti, tj;        // tile extent (rows, cols)
+  int nti, ntj;      // tiles per face along i and j
+  __host__ __device__ int tiles_per_face() const { return nti * ntj; }
+};
+
+}  // namespace bt

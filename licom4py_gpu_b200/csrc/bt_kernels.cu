@@ -1,0 +1,150 @@
+// bt_kernels.cu - sm_100a kernels of the barotropic duogrid solver and their launchers.
+//
+// Per RK stage two tile kernels run back to back (phase H, phase UV); each CTA
+// stages one tile of one face plus its 3-cell stencil halo in shared memory
+// (cross-shaped region, corners skipped), computes the C/D-grid face
+// quantities once per face and the cell updates from them.  The whole
+// member (6 faces) is one launch; halos across face edges are gathered
+// inside the tile loader (bt_stencil.cuh), so no separate exchange kernel
+// runs between phases.
+
+#include "bt_launch.cuh"
+
+namespace bt {
+
+constexpr int kThreads = 256;
+
+template <typename T, int TI, int TJ>
+__global__ void __launch_bounds__(kThreads) k_phase_h(Geo<T> g, StageIO<T> io, Tiling t) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const TileBox b = tile_box(t, g.n, blockIdx.x);
+  tile_h<T, TI, TJ>(g, io, b, reinterpret_cast<T*>(smraw));
+}
+
+template <typename T, int TI, int TJ>
+__global__ void __launch_bounds__(kThreads) k_phase_uv(Geo<T> g, StageIO<T> io, Tiling t) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const TileBox b = tile_box(t, g.n, blockIdx.x);
+  tile_uv<T, TI, TJ>(g, io, b, reinterpret_cast<T*>(smraw));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_fill_halo(Geo<T> g, T* h, T* u, T* v) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < 6 * g.nh) fill_halo_cell(g, h, u, v, k);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_diag(Geo<T> g, const T* h, const T* u, const T* v,
+                                                   DiagOut<T> d) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = g.m;
+  if (k >= 6 * m * m) return;
+  const int f = k / (m * m);
+  const int r = k - f * m * m;
+  diag_cell(g, h, u, v, d, f, r / m, r % m);
+}
+
+bool tile_cfg_supported(TileCfg c) {
+  return (c.tj == 32 && (c.ti == 4 || c.ti == 8 || c.ti == 16)) ||
+         (c.tj == 16 && (c.ti == 8 || c.ti == 16));
+}
+
+Tiling make_tiling(TileCfg c, int n) {
+  Tiling t;
+  t.ti = c.ti;
+  t.tj = c.tj;
+  t.nti = (n + c.ti - 1) / c.ti;
+  t.ntj = (n + c.tj - 1) / c.tj;
+  return t;
+}
+
+namespace {
+
+template <typename T, int TI, int TJ, bool UV>
+size_t tile_smem() {
+  using S = TileShape<TI, TJ>;
+  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH);
+}
+
+// Opt in to more than 48 KB of dynamic shared memory (done at plan creation,
+// never during stream capture).
+template <typename T, int TI, int TJ>
+cudaError_t prime_tile() {
+  cudaError_t e = cudaFuncSetAttribute(k_phase_h<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)tile_smem<T, TI, TJ, false>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_phase_uv<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)tile_smem<T, TI, TJ, true>());
+}
+
+template <typename T, int TI, int TJ, bool UV>
+cudaError_t launch_tile(const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
+  const size_t smem = tile_smem<T, TI, TJ, UV>();
+  auto kern = UV ? k_phase_uv<T, TI, TJ> : k_phase_h<T, TI, TJ>;
+  const Tiling t = make_tiling({TI, TJ}, g.n);
+  kern<<<6 * t.tiles_per_face(), kThreads, smem, s>>>(g, io, t);
+  return cudaGetLastError();
+}
+
+template <typename T, bool UV>
+cudaError_t dispatch(const Geo<T>& g, const StageIO<T>& io, TileCfg c, cudaStream_t s) {
+  if (c.tj == 32) {
+    if (c.ti == 4) return launch_tile<T, 4, 32, UV>(g, io, s);
+    if (c.ti == 8) return launch_tile<T, 8, 32, UV>(g, io, s);
+    if (c.ti == 16) return launch_tile<T, 16, 32, UV>(g, io, s);
+  } else if (c.tj == 16) {
+    if (c.ti == 8) return launch_tile<T, 8, 16, UV>(g, io, s);
+    if (c.ti == 16) return launch_tile<T, 16, 16, UV>(g, io, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t prime_kernels() {
+  cudaError_t e;
+  if ((e = prime_tile<T, 4, 32>()) != cudaSuccess) return e;
+  if ((e = prime_tile<T, 8, 32>()) != cudaSuccess) return e;
+  if ((e = prime_tile<T, 16, 32>()) != cudaSuccess) return e;
+  if ((e = prime_tile<T, 8, 16>()) != cudaSuccess) return e;
+  return prime_tile<T, 16, 16>();
+}
+
+template <typename T>
+cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s) {
+  return dispatch<T, false>(g, io, cfg, s);
+}
+
+template <typename T>
+cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s) {
+  return dispatch<T, true>(g, io, cfg, s);
+}
+
+template <typename T>
+cudaError_t launch_fill_halo(const Geo<T>& g, T* h, T* u, T* v, cudaStream_t s) {
+  const int total = 6 * g.nh;
+  k_fill_halo<T><<<(total + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, h, u, v);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_diag(const Geo<T>& g, const T* h, const T* u, const T* v, const DiagOut<T>& d,
+                        cudaStream_t s) {
+  const int total = 6 * g.m * g.m;
+  k_diag<T><<<(total + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, h, u, v, d);
+  return cudaGetLastError();
+}
+
+#define BT_INSTANTIATE(T)                                                                           \
+  template cudaError_t prime_kernels<T>();                                                          \
+  template cudaError_t launch_phase_h<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t);  \
+  template cudaError_t launch_phase_uv<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t); \
+  template cudaError_t launch_fill_halo<T>(const Geo<T>&, T*, T*, T*, cudaStream_t);                \
+  template cudaError_t launch_diag<T>(const Geo<T>&, const T*, const T*, const T*, const DiagOut<T>&, \
+                                      cudaStream_t);
+BT_INSTANTIATE(float)
+BT_INSTANTIATE(double)
+
+}  // namespace bt

@@ -1,0 +1,31 @@
+// bt_launch.cuh - host-side launch interface of the barotropic kernels (internal C++).
+#pragma once
+
+#include "bt_common.cuh"
+#include "bt_stencil.cuh"
+
+namespace bt {
+
+struct TileCfg {
+  int ti, tj;
+};
+
+// Tile shapes compiled into the library (rows x columns of interior cells).
+bool tile_cfg_supported(TileCfg c);
+Tiling make_tiling(TileCfg c, int n);
+
+// Set kernel attributes (dynamic shared memory opt-in) for the current device.
+template <typename T>
+cudaError_t prime_kernels();
+template <typename T>
+cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s);
+template <typename T>
+cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s);
+// Materialise the halo cells of h (scalar) and/or (u, v) (vector) from their interiors.
+template <typename T>
+cudaError_t launch_fill_halo(const Geo<T>& g, T* h, T* u, T* v, cudaStream_t s);
+template <typename T>
+cudaError_t launch_diag(const Geo<T>& g, const T* h, const T* u, const T* v, const DiagOut<T>& d,
+                        cudaStream_t s);
+
+}  // namespace bt
