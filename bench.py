@@ -1,0 +1,389 @@
+"""Benchmark of the barotropic RK2 path on the cubed-sphere duogrid (one JSON line).
+
+Workload (one "step" = one call of the hot path): the plain drop-in
+``_barotr_rk2_core`` round of ``--nbb`` substeps (default 1000) at C``--n``
+(default C96: 6 x 96 x 96 cells + 3-cell halos) in float64, on seeded
+synthetic fields: resting ocean of depth H = 5000 m, SSH perturbation = sum of
+real spherical harmonics l = 1..8 scaled to 1 m RMS, lon/lat velocity the same
+way at 0.3 m/s RMS, dtb at CFL 0.5 of sqrt(gH).
+
+Metric: interior cell-updates per second (one cell advanced one substep of
+two RK stages), whole job.  ``value`` is measured with inputs resident in HBM;
+``e2e`` through the public call with host (pinned) buffers, host<->device
+copies inside the timed region.  Between timed steps L2 is flushed by writing
+a 512 MiB buffer (outside the per-step CUDA-event windows).
+
+``--impl reference`` times the CPU implementation of the path instead (the
+float64 oracle, which restates the reference's source bit for bit) on the
+host cores, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): replicas only, each rank integrates its own member; no
+collective touches the data path.  Time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALG_WORDS = 41  # algorithmic words per cell-update (both RK stages), see DESIGN.md
+METRIC = "barotropic cell-updates/s"
+UNIT = "cell-updates/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=96)
+    p.add_argument("--nbb", type=int, default=1000)
+    p.add_argument("--depth", type=float, default=5000.0)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--mode", default="auto", choices=["auto", "persistent", "graph", "stream"])
+    p.add_argument("--tile", default="auto")
+    p.add_argument("--cpu-substeps", type=int, default=60,
+                   help="substeps of the bounded CPU baseline sample")
+    p.add_argument("--no-extras", action="store_true", help="skip the fp32 / mode comparison lines")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_problem(n, depth, seed):
+    from licom4py_gpu_b200 import duogrid_gen
+    from licom4py_gpu_b200.duogrid import make_consts
+    from licom4py_gpu_b200.fields import cfl_dtb, harmonic_state
+    grid = duogrid_gen.generate(n)
+    consts = make_consts(grid, depth)
+    st = harmonic_state(grid, seed)
+    dtb = cfl_dtb(grid, depth)
+    return grid, consts, st, dtb
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 7 and parts[0].isdigit():
+                    rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.remove(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [int(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][1]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the float64 oracle, bit-exact to the reference's source)
+# ---------------------------------------------------------------------------
+def cpu_baseline(consts, st, dtb, n, substeps):
+    from oracle import barotr_np as O
+    m = n + 6
+    state = [st["h0"], st["h0"], st["ub"], st["vb"], st["ub"], st["vb"]] + [np.zeros((6, m, m))] * 17
+    t0 = time.perf_counter()
+    O.rk2_core(state, consts, substeps, dtb)
+    dt = time.perf_counter() - t0
+    cells = 6 * n * n
+    return {"value": cells * substeps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"C{n} float64, {substeps} RK2 substeps from the same initial state "
+                      f"({dt:.1f} s, single-threaded NumPy oracle)"}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU implementation of the path, rank 0 only."""
+    if rank != 0:
+        return
+    _, consts, st, dtb = build_problem(args.n, args.depth, args.seed)
+    sub = max(1, args.cpu_substeps // max(1, args.steps))
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(consts, st, dtb, args.n, 1)
+    vals, t_total = [], 0.0
+    for _ in range(args.steps):
+        r = cpu_baseline(consts, st, dtb, args.n, sub)
+        vals.append(r["value"])
+        t_total += 6 * args.n * args.n * sub / r["value"]
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic seeded spherical-harmonic fields",
+            "config": {"workload": f"C{args.n} plain RK2, {sub} substeps per step (bounded sample of "
+                                   f"the {args.nbb}-substep round), float64", "n": args.n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"{sub} substeps per step x {args.steps} steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+    from licom4py_gpu_b200 import barotr
+    from licom4py_gpu_b200.plan import DIAG_NAMES, BtPlan
+    from licom4py_gpu_b200.autotune import choose_config
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    grid, consts, st, dtb = build_problem(args.n, args.depth, args.seed + rank)
+    n, m, nbb = args.n, args.n + 6, args.nbb
+    cells = 6 * n * n
+
+    def dev_state(dtype):
+        h = torch.from_numpy(st["h0"]).to(dev, dtype)
+        u = torch.from_numpy(st["ub"]).to(dev, dtype)
+        v = torch.from_numpy(st["vb"]).to(dev, dtype)
+        return [h, h, u, v, u, v]
+
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def timed_rounds(plan, ins, out, steps, warmup, kernel_timing=False):
+        for _ in range(warmup):
+            plan.round(*ins, nbb=nbb, dtb=dtb, out=out)
+        torch.cuda.synchronize()
+        if kernel_timing:
+            plan.enable_kernel_timing(True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        barrier(world)
+        torch.cuda.synchronize()
+        for k in range(steps):
+            flush.fill_(float(k))
+            ev[k][0].record()
+            plan.round(*ins, nbb=nbb, dtb=dtb, out=out)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        kt = plan.kernel_time() if kernel_timing else (0.0, 0)
+        if kernel_timing:
+            plan.enable_kernel_timing(False)
+        return ms, kt
+
+    def make_plan(dtype, mode, tile):
+        p = BtPlan(consts, dtype=dtype, device=dev, tile=tile, mode=mode)
+        return p
+
+    # configuration: autotuned (mode, tile) unless given
+    cfg = choose_config(n, torch.float64, consts=consts, device=dev) if (args.mode == "auto" or args.tile == "auto") else None
+    mode = cfg["mode"] if args.mode == "auto" else args.mode
+    tile = tuple(cfg["tile"]) if args.tile == "auto" else tuple(int(x) for x in args.tile.split("x"))
+
+    ins64 = dev_state(torch.float64)
+    plan = make_plan(torch.float64, mode, tile)
+    out = {k: plan.empty_field() for k in ("h0", "ub", "vb") + DIAG_NAMES}
+    sampler = ClockSampler(local)
+    with sampler:
+        ms, (kms, klaunch) = timed_rounds(plan, ins64, out, args.steps, args.warmup,
+                                          kernel_timing=(mode == "persistent"))
+    clocks = sampler.summary()
+    ms = max_over_ranks(ms, world)
+    ms_per_step = ms / args.steps
+    value = world * cells * nbb * args.steps / (ms * 1e-3)
+    launches_per_step = {"persistent": 4, "graph": 4 * nbb + 3, "stream": 4 * nbb + 3}[mode]
+
+    # roofline of the dominant kernel (the persistent round kernel: one launch per step)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    roofline = None
+    if mode == "persistent" and klaunch:
+        alg_bytes = B_ALG_WORDS * 8 * cells * nbb
+        achieved = alg_bytes / (kms / klaunch * 1e-3) / 1e9
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", f"k_round_c{n}_f64_traffic.json")
+        if os.path.exists(tfile):
+            try:
+                tj = json.load(open(tfile))
+                traffic = tj.get("dram_bytes_per_launch_scaled", {}).get(str(nbb))
+            except (OSError, ValueError):
+                traffic = None
+        roofline = {"bound": "hbm", "kernel": "k_round<double>", "achieved": achieved, "peak": peak,
+                    "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                    "kernel_ms": kms / klaunch, "alg_bytes_per_launch": alg_bytes}
+
+    # end to end through the public call, host (pinned) buffers
+    pinned_in = [torch.from_numpy(a).pin_memory() for a in (st["h0"], st["h0"], st["ub"], st["vb"], st["ub"], st["vb"])]
+    dev_in = [torch.empty((6, m, m), dtype=torch.float64, device=dev) for _ in range(6)]
+    pinned_out = [torch.empty((6, m, m), dtype=torch.float64).pin_memory() for _ in range(13)]
+    zeros = [torch.zeros((6, m, m), dtype=torch.float64, device=dev) for _ in range(17)]
+    core_plan = barotr.get_plan(consts, dtype=torch.float64, device=dev)
+    core_plan.set_mode(mode)
+    core_plan.set_tile(*tile)
+
+    def e2e_step():
+        for d, h in zip(dev_in, pinned_in):
+            d.copy_(h, non_blocking=True)
+        state = tuple(dev_in) + tuple(zeros)
+        res = barotr._barotr_rk2_core(state, consts, nbb, dtb, 1, 1)
+        outs = [res[0], res[2], res[3]] + list(res[6:16])
+        for h, d in zip(pinned_out, outs):
+            h.copy_(d, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    e2e = {"value": world * cells * nbb * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": sum(t.numel() * t.element_size() for t in pinned_in),
+           "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in pinned_out),
+           "ms_per_step": e2e_ms / args.steps}
+
+    extras = {}
+    if not args.no_extras:
+        # float32 precision form, same workload
+        ins32 = dev_state(torch.float32)
+        p32 = make_plan(torch.float32, mode, tile)
+        out32 = {k: p32.empty_field() for k in ("h0", "ub", "vb") + DIAG_NAMES}
+        ms32, _ = timed_rounds(p32, ins32, out32, args.steps, args.warmup)
+        ms32 = max_over_ranks(ms32, world)
+        h64 = out["h0"][:, 3:-3, 3:-3]
+        h32 = out32["h0"][:, 3:-3, 3:-3].double()
+        extras["fp32"] = {"value": world * cells * nbb * args.steps / (ms32 * 1e-3), "unit": UNIT,
+                          "ms_per_step": ms32 / args.steps,
+                          "h_rel_l2_vs_f64": float((h32 - h64).norm() / h64.norm())}
+        p32.close()
+        # round execution modes (CUDA graph vs persistent vs stream), float64
+        modes = {}
+        for md in ("persistent", "graph", "stream"):
+            pm = make_plan(torch.float64, md, tile)
+            steps = max(2, args.steps // 2)
+            msm, _ = timed_rounds(pm, ins64, out, steps, 2)
+            modes[md] = {"value": cells * nbb * steps / (msm * 1e-3), "ms_per_step": msm / steps}
+            pm.close()
+        extras["modes_f64"] = modes
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(consts, st, dtb, n, args.cpu_substeps)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic: seeded spherical harmonics l=1..8 (h 1 m RMS, u/v 0.3 m/s RMS) over H=5000 m",
+                "config": {"workload": f"C{n} plain drop-in RK2 round, {nbb} substeps per step, float64",
+                           "n": n, "nbb": nbb, "rk": 2, "dtb_s": dtb, "mode": mode, "tile": list(tile),
+                           "parallelism": f"replicas x{world}",
+                           "l2": "flushed between steps (512 MiB write outside the timed windows); "
+                                 "within a step the member's working set stays L2-resident"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    plan.close()
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

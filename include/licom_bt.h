@@ -44,6 +44,15 @@ extern "C" {
 #define BT_MODE_GRAPH 1       /* the round is captured once as a CUDA graph and replayed */
 #define BT_MODE_PERSISTENT 2  /* one cooperative launch with grid barriers per round */
 
+/* Plan options (bt_plan_set_option) */
+#define BT_OPT_MAX_CTAS 1    /* persistent mode: cap on the cooperative grid (0 = occupancy limit) */
+#define BT_OPT_SPIN_LIMIT 2  /* persistent mode: polls a grid-barrier wait may take before it gives up */
+#define BT_OPT_KERNEL_TIMING 3  /* persistent mode: 1 = bracket each round kernel with CUDA events */
+
+/* Plan information (bt_plan_get_info) */
+#define BT_INFO_LAST_GRID 1      /* CTAs of the last persistent launch */
+#define BT_INFO_SCRATCH_BYTES 2  /* device scratch owned by the plan */
+
 typedef struct bt_plan bt_plan;
 
 /* Geometry of one resolution: the 17 constants in CONST_SOURCES order
@@ -106,6 +115,18 @@ int bt_plan_destroy(bt_plan* plan);
 /* Tile shape (rows ti x columns tj of interior cells per CTA) and round mode. */
 int bt_plan_set_tile(bt_plan* plan, int ti, int tj);
 int bt_plan_set_mode(bt_plan* plan, int mode);
+
+/* Set a plan option (BT_OPT_*).  A barrier wait that exceeds BT_OPT_SPIN_LIMIT
+ * polls sets the plan's device error flag and ends the round early instead of
+ * waiting forever; bt_check_device_error then reports BT_EDEVICE. */
+int bt_plan_set_option(bt_plan* plan, int key, long long value);
+
+/* Sum of the durations of the round kernels launched since timing was
+ * enabled or last read (BT_OPT_KERNEL_TIMING); waits for them; resets the sum. */
+int bt_plan_kernel_time(bt_plan* plan, double* ms_total, int* launches);
+
+/* Read plan information (BT_INFO_*); -1 for an unknown key. */
+long long bt_plan_get_info(bt_plan* plan, int key);
 
 /* Advance nbb (>= 1) substeps of RK2 (rk = 2, midpoint, barotr.py:41-61) or
  * RK3 (rk = 3, barotr.py:64-87) with step dtb.  Replaces the call

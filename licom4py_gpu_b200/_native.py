@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libbt.so")
 BT_OK, BT_EINVAL, BT_ENOMEM, BT_ECUDA, BT_EDEVICE, BT_ENOTSUP = 0, -1, -2, -3, -4, -5
 BT_F64, BT_F32 = 0, 1
 BT_MODE_STREAM, BT_MODE_GRAPH, BT_MODE_PERSISTENT = 0, 1, 2
+BT_OPT_MAX_CTAS, BT_OPT_SPIN_LIMIT, BT_OPT_KERNEL_TIMING = 1, 2, 3
+BT_INFO_LAST_GRID, BT_INFO_SCRATCH_BYTES = 1, 2
 
 _vp = ctypes.c_void_p
 
@@ -41,7 +43,8 @@ class BtError(RuntimeError):
 _lib = None
 
 # every symbol declared in include/licom_bt.h
-EXPORTS = ("bt_plan_create", "bt_plan_destroy", "bt_plan_set_tile", "bt_plan_set_mode", "bt_round",
+EXPORTS = ("bt_plan_create", "bt_plan_destroy", "bt_plan_set_tile", "bt_plan_set_mode",
+           "bt_plan_set_option", "bt_plan_get_info", "bt_plan_kernel_time", "bt_round",
            "bt_stage", "bt_fill_halo", "bt_edge_average", "bt_check_device_error", "bt_halo_table_host", "bt_last_error", "bt_version")
 
 
@@ -59,6 +62,9 @@ def lib():
     L.bt_plan_destroy.argtypes = [_vp]
     L.bt_plan_set_tile.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.bt_plan_set_mode.argtypes = [_vp, ctypes.c_int]
+    L.bt_plan_set_option.argtypes = [_vp, ctypes.c_int, ctypes.c_longlong]
+    L.bt_plan_get_info.argtypes = [_vp, ctypes.c_int]
+    L.bt_plan_kernel_time.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     L.bt_round.argtypes = [_vp, ctypes.POINTER(StateIn), ctypes.POINTER(StateOut), ctypes.c_int,
                            ctypes.c_double, ctypes.c_int, _vp]
     L.bt_stage.argtypes = [_vp, ctypes.POINTER(StateIn), ctypes.POINTER(StateOut), ctypes.c_double,
@@ -73,6 +79,7 @@ def lib():
     for name in EXPORTS:
         if name != "bt_last_error":
             getattr(L, name).restype = ctypes.c_int
+    L.bt_plan_get_info.restype = ctypes.c_longlong
     _lib = L
     return L
 

@@ -1,0 +1,111 @@
+"""Autotuner for the round execution mode and tile shape.
+
+For one resolution N and dtype it times short rounds of every candidate
+(mode in {persistent, graph}) x (tile shape) on the current GPU and keeps the
+fastest.  Results are cached per (GPU name, N, dtype) in a JSON file
+(``$LICOM_BT_TUNE_CACHE``, default ``~/.cache/licom4py_gpu_b200/tune.json``).
+Without constants to time with, a static heuristic is returned.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+from typing import Dict, Optional, Sequence
+
+import torch
+
+TILES = ((4, 32), (8, 32), (16, 32), (8, 16), (16, 16))
+MODES = ("persistent", "graph")
+
+
+def _cache_path() -> str:
+    return os.environ.get("LICOM_BT_TUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "licom4py_gpu_b200", "tune.json"))
+
+
+def _load_cache() -> Dict[str, dict]:
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(key: str, cfg: dict) -> None:
+    cache = _load_cache()
+    cache[key] = cfg
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(cache, f, indent=1)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
+def heuristic(n: int) -> dict:
+    """Static choice: small grids are barrier/launch bound -> persistent; large ones graph."""
+    if n <= 64:
+        return {"mode": "persistent", "tile": [8, 16], "source": "heuristic"}
+    if n <= 192:
+        return {"mode": "persistent", "tile": [8, 32], "source": "heuristic"}
+    return {"mode": "graph", "tile": [16, 32], "source": "heuristic"}
+
+
+def _key(n: int, dtype: torch.dtype, device) -> str:
+    name = torch.cuda.get_device_name(device)
+    return f"{name}|C{n}|{str(dtype).replace('torch.', '')}"
+
+
+def tune(n: int, dtype: torch.dtype, consts: Sequence, device=None, nbb: int = 40, reps: int = 3,
+         modes: Sequence[str] = MODES, tiles: Sequence = TILES) -> dict:
+    """Time every (mode, tile) candidate on ``nbb``-substep rounds; return and cache the best."""
+    from .fields import harmonic_state  # noqa: F401  (keeps the import graph explicit)
+    from .plan import BtPlan
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    m = n + 6
+    g = torch.Generator(device="cpu").manual_seed(0)
+    h = (torch.randn((6, m, m), generator=g, dtype=torch.float64) * 0.5).to(dev, dtype)
+    u = (torch.randn((6, m, m), generator=g, dtype=torch.float64) * 0.1).to(dev, dtype)
+    v = (torch.randn((6, m, m), generator=g, dtype=torch.float64) * 0.1).to(dev, dtype)
+    ins = [h, h, u, v, u, v]
+    dtb = 0.05 * 1.231 * 6.3712e6 / n / (9.8 * 5000.0) ** 0.5  # small, stable step for timing
+    results = []
+    for mode in modes:
+        for tile in tiles:
+            p = BtPlan(consts, dtype=dtype, device=dev, tile=tile, mode=mode)
+            out = None
+            try:
+                out = p.round(*ins, nbb=nbb, dtb=dtb, diag=False)
+                torch.cuda.synchronize(dev)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                for _ in range(reps):
+                    p.round(*ins, nbb=nbb, dtb=dtb, diag=False, out=out)
+                b.record()
+                torch.cuda.synchronize(dev)
+                ms = a.elapsed_time(b) / reps
+                results.append({"mode": mode, "tile": list(tile), "ms_per_round": ms,
+                                "cell_updates_per_s": 6 * n * n * nbb / (ms * 1e-3)})
+            finally:
+                p.close()
+    best = min(results, key=lambda r: r["ms_per_round"])
+    cfg = {"mode": best["mode"], "tile": best["tile"], "source": "tuned", "nbb": nbb, "candidates": results}
+    _store(_key(n, dtype, dev), cfg)
+    return cfg
+
+
+def choose_config(n: int, dtype: torch.dtype = torch.float64, consts: Optional[Sequence] = None,
+                  device=None, retune: bool = False) -> dict:
+    """Cached tuned config, else tune when constants are given, else the heuristic."""
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if not retune:
+        cfg = _load_cache().get(_key(n, dtype, dev))
+        if cfg is not None:
+            return cfg
+    if consts is None:
+        return heuristic(n)
+    return tune(n, dtype, consts, dev)

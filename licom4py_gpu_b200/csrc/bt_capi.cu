@@ -95,6 +95,15 @@ struct bt_plan {
   // graph cache
   cudaGraphExec_t gexec = nullptr;
   std::vector<uintptr_t> gkey;
+  // persistent mode: barrier counter + device error flag, options
+  unsigned* d_flags = nullptr;  // [0] barrier counter, [1] error bits
+  int max_ctas = 0;
+  long long spin_limit = 1ll << 24;
+  int last_grid = 0;
+  // optional timing of the main round kernel (persistent mode): event pairs on the launch stream
+  int timing = 0;
+  std::vector<cudaEvent_t> tev;
+  size_t tev_used = 0;
 
   size_t esize() const { return dtype == BT_F64 ? 8 : 4; }
   void* scratch_field(int k) const { return (char*)scratch + (size_t)k * field_elems * esize(); }
@@ -314,6 +323,62 @@ cudaError_t enqueue_stage(const bt_plan* p, const bt_state_in& in, const bt_stat
   return launch_fill_halo<T>(g, X[0], X[1], X[2], s);
 }
 
+// Persistent mode: one cooperative launch runs every phase of every substep.
+template <typename T>
+cudaError_t enqueue_round_persistent(bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb,
+                                     double dtb, int rk, cudaStream_t s) {
+  RoundArgs<T> a;
+  a.g = p->geo<T>();
+  for (int k = 0; k < 3; ++k) {
+    a.y[k] = (T*)p->scratch_field(k);
+    a.z[k] = (T*)p->scratch_field(3 + k);
+  }
+  a.x0[0] = (const T*)in.h0;
+  a.x0[1] = (const T*)in.ub;
+  a.x0[2] = (const T*)in.vb;
+  a.b0[0] = (const T*)in.h0p;
+  a.b0[1] = (const T*)in.ubp;
+  a.b0[2] = (const T*)in.vbp;
+  a.x[0] = (T*)out.h0;
+  a.x[1] = (T*)out.ub;
+  a.x[2] = (T*)out.vb;
+  a.nbb = nbb;
+  a.rk = rk;
+  a.dtb = dtb;
+  a.bar = p->d_flags;
+  a.err = (int*)(p->d_flags + 1);
+  a.spin_limit = p->spin_limit;
+  cudaError_t e = cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (p->timing) {
+    if (p->tev_used + 2 > p->tev.size()) {
+      for (int k = 0; k < 2; ++k) {
+        cudaEvent_t ev;
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+        p->tev.push_back(ev);
+      }
+    }
+    t0 = p->tev[p->tev_used];
+    t1 = p->tev[p->tev_used + 1];
+    p->tev_used += 2;
+    if ((e = cudaEventRecord(t0, s)) != cudaSuccess) return e;
+  }
+  e = launch_round<T>(a, p->tile, p->max_ctas, s, &p->last_grid);
+  if (e != cudaSuccess) return e;
+  if (t1 && (e = cudaEventRecord(t1, s)) != cudaSuccess) return e;
+  const Geo<T>& g = a.g;
+  if (out.diag[0]) {
+    T* const* L = rk == 2 ? a.y : a.z;
+    if ((e = launch_fill_halo<T>(g, L[0], L[1], L[2], s)) != cudaSuccess) return e;
+    DiagOut<T> d;
+    T** dp = (T**)&d;
+    for (int k = 0; k < 10; ++k) dp[k] = (T*)out.diag[k];
+    if ((e = launch_diag<T>(g, L[0], L[1], L[2], d, s)) != cudaSuccess) return e;
+  }
+  return launch_fill_halo<T>(g, a.x[0], a.x[1], a.x[2], s);
+}
+
 cudaError_t enqueue(const bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb, double dtb,
                     int rk, cudaStream_t s) {
   return p->dtype == BT_F64 ? enqueue_round<double>(p, in, out, nbb, dtb, rk, s)
@@ -413,6 +478,12 @@ int bt_plan_create(const bt_grid_desc* d, bt_plan** out) {
     bt_plan_destroy(p);
     return fail(BT_ENOMEM, std::string("bt_plan_create: scratch allocation: ") + cudaGetErrorString(e));
   }
+  e = cudaMalloc(&p->d_flags, 2 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(p->d_flags, 0, 2 * sizeof(unsigned));
+  if (e != cudaSuccess) {
+    bt_plan_destroy(p);
+    return fail(BT_ENOMEM, std::string("bt_plan_create: flag allocation: ") + cudaGetErrorString(e));
+  }
   e = cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming);
@@ -429,8 +500,10 @@ int bt_plan_destroy(bt_plan* p) {
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
   if (p->ev_in) cudaEventDestroy(p->ev_in);
   if (p->ev_out) cudaEventDestroy(p->ev_out);
+  for (cudaEvent_t ev : p->tev) cudaEventDestroy(ev);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   if (p->scratch) cudaFree(p->scratch);
+  if (p->d_flags) cudaFree(p->d_flags);
   if (p->d_hsrc) cudaFree(p->d_hsrc);
   if (p->d_hw) cudaFree(p->d_hw);
   delete p;
@@ -451,8 +524,8 @@ int bt_plan_set_tile(bt_plan* p, int ti, int tj) {
 
 int bt_plan_set_mode(bt_plan* p, int mode) {
   if (!p) return fail(BT_EINVAL, "bt_plan_set_mode: NULL plan");
-  if (mode != BT_MODE_STREAM && mode != BT_MODE_GRAPH)
-    return fail(BT_ENOTSUP, "bt_plan_set_mode: mode not available in this build");
+  if (mode != BT_MODE_STREAM && mode != BT_MODE_GRAPH && mode != BT_MODE_PERSISTENT)
+    return fail(BT_EINVAL, "bt_plan_set_mode: unknown mode");
   p->mode = mode;
   return BT_OK;
 }
@@ -473,6 +546,12 @@ int bt_round(bt_plan* p, const bt_state_in* in, const bt_state_out* out, int nbb
     for (int k = 1; k < 10; ++k)
       if (!out->diag[k]) return fail(BT_EINVAL, "bt_round: diag outputs must be all set or diag[0] NULL");
   cudaStream_t s = (cudaStream_t)stream;
+  if (p->mode == BT_MODE_PERSISTENT) {
+    cudaError_t e = p->dtype == BT_F64 ? enqueue_round_persistent<double>(p, *in, *out, nbb, dtb, rk, s)
+                                       : enqueue_round_persistent<float>(p, *in, *out, nbb, dtb, rk, s);
+    if (e != cudaSuccess) return cuda_fail(e, "bt_round: persistent launch");
+    return BT_OK;
+  }
   if (p->mode == BT_MODE_STREAM) {
     cudaError_t e = enqueue(p, *in, *out, nbb, dtb, rk, s);
     if (e != cudaSuccess) return cuda_fail(e, "bt_round: launch");
@@ -555,7 +634,59 @@ int bt_edge_average(bt_plan* p, void* u, void* v, void* stream) {
 int bt_check_device_error(bt_plan* p) {
   if (!p) return fail(BT_EINVAL, "bt_check_device_error: NULL plan");
   BT_CUDA(cudaDeviceSynchronize(), "bt_check_device_error: synchronize");
+  unsigned flags[2];
+  BT_CUDA(cudaMemcpy(flags, p->d_flags, sizeof(flags), cudaMemcpyDeviceToHost), "bt_check_device_error: read flag");
+  if (flags[1] != 0) {
+    BT_CUDA(cudaMemset(p->d_flags + 1, 0, sizeof(unsigned)), "bt_check_device_error: clear flag");
+    if (flags[1] & kErrBarrierTimeout)
+      return fail(BT_EDEVICE, "persistent round: grid barrier wait exceeded its poll limit; the round was abandoned");
+    return fail(BT_EDEVICE, "device error flag " + std::to_string(flags[1]));
+  }
   return BT_OK;
+}
+
+int bt_plan_set_option(bt_plan* p, int key, long long value) {
+  if (!p) return fail(BT_EINVAL, "bt_plan_set_option: NULL plan");
+  switch (key) {
+    case BT_OPT_MAX_CTAS:
+      if (value < 0 || value > (1 << 20)) return fail(BT_EINVAL, "bt_plan_set_option: max_ctas out of range");
+      p->max_ctas = (int)value;
+      return BT_OK;
+    case BT_OPT_SPIN_LIMIT:
+      if (value < -1) return fail(BT_EINVAL, "bt_plan_set_option: spin limit must be >= -1");
+      p->spin_limit = value;
+      return BT_OK;
+    case BT_OPT_KERNEL_TIMING:
+      p->timing = value ? 1 : 0;
+      p->tev_used = 0;
+      return BT_OK;
+    default:
+      return fail(BT_EINVAL, "bt_plan_set_option: unknown option");
+  }
+}
+
+int bt_plan_kernel_time(bt_plan* p, double* ms_total, int* launches) {
+  if (!p || !ms_total || !launches) return fail(BT_EINVAL, "bt_plan_kernel_time: NULL argument");
+  double total = 0.0;
+  for (size_t k = 0; k + 1 < p->tev_used; k += 2) {
+    BT_CUDA(cudaEventSynchronize(p->tev[k + 1]), "bt_plan_kernel_time: synchronize");
+    float ms = 0.f;
+    BT_CUDA(cudaEventElapsedTime(&ms, p->tev[k], p->tev[k + 1]), "bt_plan_kernel_time: elapsed");
+    total += ms;
+  }
+  *ms_total = total;
+  *launches = (int)(p->tev_used / 2);
+  p->tev_used = 0;
+  return BT_OK;
+}
+
+long long bt_plan_get_info(bt_plan* p, int key) {
+  if (!p) return -1;
+  switch (key) {
+    case BT_INFO_LAST_GRID: return p->last_grid;
+    case BT_INFO_SCRATCH_BYTES: return (long long)((6 * p->field_elems + 24 * (size_t)p->n) * p->esize());
+    default: return -1;
+  }
 }
 
 }  // extern "C"

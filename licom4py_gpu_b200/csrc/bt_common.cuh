@@ -92,11 +92,34 @@ struct StageIO {
   int last;         // 1: last stage of the substep (mass-flux edge average active)
 };
 
+// Error bits a kernel can raise in the plan's device flag.
+enum DeviceError { kErrBarrierTimeout = 1 };
+
+// Everything one persistent launch needs to run a whole round of one member.
+template <typename T>
+struct RoundArgs;
+
 // Tile decomposition of the N x N interior of each face.
 struct Tiling {
   int ti, tj;        // tile extent (rows, cols)
   int nti, ntj;      // tiles per face along i and j
   __host__ __device__ int tiles_per_face() const { return nti * ntj; }
+};
+
+template <typename T>
+struct RoundArgs {
+  Geo<T> g;
+  Tiling t;
+  const T* x0[3];  // round input h0, ub, vb (halos valid)
+  const T* b0[3];  // round input base h0p, ubp, vbp
+  T* x[3];         // output / running state
+  T* y[3];         // stage scratch
+  T* z[3];         // second stage scratch (RK3)
+  int nbb, rk;
+  double dtb;
+  unsigned* bar;   // grid barrier counter, zero at launch
+  int* err;        // device error flag
+  long long spin_limit;
 };
 
 }  // namespace bt

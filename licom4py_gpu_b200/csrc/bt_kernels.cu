@@ -8,6 +8,8 @@
 // inside the tile loader (bt_stencil.cuh), so no separate exchange kernel
 // runs between phases.
 
+#include <algorithm>
+
 #include "bt_launch.cuh"
 
 namespace bt {
@@ -26,6 +28,32 @@ __global__ void __launch_bounds__(kThreads) k_phase_uv(Geo<T> g, StageIO<T> io, 
   extern __shared__ __align__(16) unsigned char smraw[];
   const TileBox b = tile_box(t, g.n, blockIdx.x);
   tile_uv<T, TI, TJ>(g, io, b, reinterpret_cast<T*>(smraw));
+}
+
+// One whole round of one member in a single cooperative launch: every CTA
+// walks the tiles of a phase, then all CTAs meet at a grid barrier.
+template <typename T, int TI, int TJ>
+__global__ void __launch_bounds__(kThreads) k_round(RoundArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
+  const int ntiles = 6 * a.t.tiles_per_face();
+  const int nst = a.rk == 2 ? 2 : 3;
+  unsigned gen = 0;
+  for (int step = 0; step < a.nbb; ++step) {
+    for (int st = 0; st < nst; ++st) {
+      const StageIO<T> io = round_stage(a, step, st);
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        tile_h<T, TI, TJ>(a.g, io, tile_box(a.t, a.g.n, tile), sm);
+        __syncthreads();
+      }
+      if (!grid_barrier(a.bar, gen, a.err, a.spin_limit)) return;
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        tile_uv<T, TI, TJ>(a.g, io, tile_box(a.t, a.g.n, tile), sm);
+        __syncthreads();
+      }
+      if (!grid_barrier(a.bar, gen, a.err, a.spin_limit)) return;
+    }
+  }
 }
 
 template <typename T>
@@ -74,8 +102,31 @@ cudaError_t prime_tile() {
   cudaError_t e = cudaFuncSetAttribute(k_phase_h<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)tile_smem<T, TI, TJ, false>());
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_round<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)tile_smem<T, TI, TJ, true>());
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_phase_uv<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)tile_smem<T, TI, TJ, true>());
+}
+
+// Co-resident grid for the persistent kernel (at most one CTA per tile).
+template <typename T, int TI, int TJ>
+cudaError_t launch_round_tile(RoundArgs<T> a, int max_ctas, cudaStream_t s, int* grid_out) {
+  const size_t smem = tile_smem<T, TI, TJ, true>();
+  int dev, sms, per_sm;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_round<T, TI, TJ>, kThreads, smem)) !=
+      cudaSuccess)
+    return e;
+  a.t = make_tiling({TI, TJ}, a.g.n);
+  int grid = std::min(per_sm * sms, 6 * a.t.tiles_per_face());
+  if (max_ctas > 0) grid = std::min(grid, max_ctas);
+  if (grid < 1) return cudaErrorInvalidConfiguration;
+  if (grid_out) *grid_out = grid;
+  void* args[] = {&a};
+  return cudaLaunchCooperativeKernel((const void*)k_round<T, TI, TJ>, dim3(grid), dim3(kThreads), args, smem, s);
 }
 
 template <typename T, int TI, int TJ, bool UV>
@@ -101,6 +152,19 @@ cudaError_t dispatch(const Geo<T>& g, const StageIO<T>& io, TileCfg c, cudaStrea
 }
 
 }  // namespace
+
+template <typename T>
+cudaError_t launch_round(const RoundArgs<T>& a, TileCfg c, int max_ctas, cudaStream_t s, int* grid_out) {
+  if (c.tj == 32) {
+    if (c.ti == 4) return launch_round_tile<T, 4, 32>(a, max_ctas, s, grid_out);
+    if (c.ti == 8) return launch_round_tile<T, 8, 32>(a, max_ctas, s, grid_out);
+    if (c.ti == 16) return launch_round_tile<T, 16, 32>(a, max_ctas, s, grid_out);
+  } else if (c.tj == 16) {
+    if (c.ti == 8) return launch_round_tile<T, 8, 16>(a, max_ctas, s, grid_out);
+    if (c.ti == 16) return launch_round_tile<T, 16, 16>(a, max_ctas, s, grid_out);
+  }
+  return cudaErrorInvalidValue;
+}
 
 template <typename T>
 cudaError_t prime_kernels() {
@@ -142,6 +206,7 @@ cudaError_t launch_diag(const Geo<T>& g, const T* h, const T* u, const T* v, con
   template cudaError_t launch_phase_h<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t);  \
   template cudaError_t launch_phase_uv<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t); \
   template cudaError_t launch_fill_halo<T>(const Geo<T>&, T*, T*, T*, cudaStream_t);                \
+  template cudaError_t launch_round<T>(const RoundArgs<T>&, TileCfg, int, cudaStream_t, int*);      \
   template cudaError_t launch_diag<T>(const Geo<T>&, const T*, const T*, const T*, const DiagOut<T>&, \
                                       cudaStream_t);
 BT_INSTANTIATE(float)

@@ -21,6 +21,10 @@ template <typename T>
 cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s);
 template <typename T>
 cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s);
+// Persistent cooperative launch of a whole round (phases of all substeps);
+// max_ctas > 0 caps the grid.  The grid size used is returned in *grid_out.
+template <typename T>
+cudaError_t launch_round(const RoundArgs<T>& a, TileCfg cfg, int max_ctas, cudaStream_t s, int* grid_out);
 // Materialise the halo cells of h (scalar) and/or (u, v) (vector) from their interiors.
 template <typename T>
 cudaError_t launch_fill_halo(const Geo<T>& g, T* h, T* u, T* v, cudaStream_t s);

@@ -413,6 +413,75 @@ __device__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
 }
 
 // ---------------------------------------------------------------------------
+// Grid-wide barrier of the persistent round kernel
+// ---------------------------------------------------------------------------
+// Monotone arrival counter: the k-th barrier completes when the counter reaches
+// k * gridDim.x.  Thread 0 of each CTA publishes the CTA's writes (fence), arrives
+// and spins with a bounded number of polls; on timeout it raises
+// kErrBarrierTimeout and every CTA leaves the round at its next barrier.
+// Returns false when the round must stop.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* err, long long limit) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ++gen;
+    const unsigned target = gen * gridDim.x;
+    __threadfence();
+    atomicAdd(bar, 1u);
+    long long polls = 0;
+    int ok = 1;
+    while (true) {
+      unsigned seen;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(bar) : "memory");
+      if ((int)(seen - target) >= 0) break;
+      if (++polls > limit) {
+        atomicOr(err, kErrBarrierTimeout);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    if (ok && *((volatile int*)err) != 0) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Stage pointers of (substep, stage) of a round; mirrors the host schedule.
+template <typename T>
+__device__ StageIO<T> round_stage(const RoundArgs<T>& a, int step, int st) {
+  StageIO<T> io;
+  const T* const* cur = step == 0 ? a.x0 : (const T* const*)a.x;
+  const T* const* base = step == 0 ? a.b0 : (const T* const*)a.x;
+  const int nst = a.rk == 2 ? 2 : 3;
+  const T* const* in = st == 0 ? cur : (st == 1 ? (const T* const*)a.y : (const T* const*)a.z);
+  T* const* out = st == nst - 1 ? a.x : (st == 0 ? a.y : a.z);
+  io.h = in[0];
+  io.u = in[1];
+  io.v = in[2];
+  io.hp = base[0];
+  io.up = base[1];
+  io.vp = base[2];
+  io.h_out = out[0];
+  io.u_out = out[1];
+  io.v_out = out[2];
+  double dt;
+  if (a.rk == 2) {
+    dt = st == 0 ? a.dtb / 2.0 : a.dtb;      // barotr.py:50-56
+    io.beta = T(0.0);
+  } else {
+    dt = st == 0 ? a.dtb / 3.0 : (st == 1 ? a.dtb / 2.0 : a.dtb);  // barotr.py:73-83
+    io.beta = T(1.0);
+  }
+  io.dt = (T)dt;
+  io.stored_halo = (step == 0 && st == 0) ? 1 : 0;
+  io.last = st == nst - 1 ? 1 : 0;
+  return io;
+}
+
+// ---------------------------------------------------------------------------
 // Materialised halos (end of a round) and diagnostics
 // ---------------------------------------------------------------------------
 // Write every halo cell of face-major field(s) from their own interior.

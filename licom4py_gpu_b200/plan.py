@@ -91,6 +91,36 @@ class BtPlan:
         N.check(N.lib().bt_plan_set_mode(self._h, _MODES[mode]))
         self.mode = mode
 
+    def set_option(self, key: int, value: int) -> None:
+        N.check(N.lib().bt_plan_set_option(self._h, int(key), int(value)))
+
+    def set_max_ctas(self, n: int) -> None:
+        """Persistent mode: cap the cooperative grid (0 = as many as fit)."""
+        self.set_option(N.BT_OPT_MAX_CTAS, n)
+
+    def set_spin_limit(self, polls: int) -> None:
+        """Persistent mode: polls a grid-barrier wait may take before the round is abandoned."""
+        self.set_option(N.BT_OPT_SPIN_LIMIT, polls)
+
+    def enable_kernel_timing(self, on: bool = True) -> None:
+        """Persistent mode: bracket every round kernel with CUDA events on its stream."""
+        self.set_option(N.BT_OPT_KERNEL_TIMING, 1 if on else 0)
+
+    def kernel_time(self) -> Tuple[float, int]:
+        """(total ms, launches) of the timed round kernels since the last read."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int()
+        N.check(N.lib().bt_plan_kernel_time(self._h, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    @property
+    def last_grid(self) -> int:
+        return int(N.lib().bt_plan_get_info(self._h, N.BT_INFO_LAST_GRID))
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(N.lib().bt_plan_get_info(self._h, N.BT_INFO_SCRATCH_BYTES))
+
     # -- validation --------------------------------------------------------------
     def _check_field(self, name: str, t: torch.Tensor) -> None:
         if not isinstance(t, torch.Tensor):

@@ -14,7 +14,7 @@ from licom4py_gpu_b200.duogrid import make_consts
 
 def _declared(header):
     text = open(os.path.join(ROOT, "include", header)).read()
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*((?:bt|ldg)_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:const\s+)?(?:unsigned\s+|long\s+)*\w+\s*\*?\s*((?:bt|ldg)_\w+)\s*\(", text, re.M)))
 
 
 def test_libbt_exports_every_declared_symbol():
