@@ -28,8 +28,12 @@ INCLUDE = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", shutil.which("g++") or "g++")
 
-CUDA_SOURCES = ["bt_kernels.cu", "bt_capi.cu"]
-CUDA_HEADERS = ["bt_common.cuh", "bt_stencil.cuh", "bt_launch.cuh"]
+# (source, extra nvcc flags): the float64 kernels and the C-ABI are built
+# without FMA contraction so float64 results round like the reference's
+# arithmetic; the float32 precision form keeps FMA.
+CUDA_SOURCES = [("bt_kernels_f64.cu", ["-fmad=false"]), ("bt_kernels_f32.cu", ["-fmad=true"]),
+                ("bt_capi.cu", ["-fmad=false"])]
+CUDA_HEADERS = ["bt_common.cuh", "bt_stencil.cuh", "bt_launch.cuh", "bt_kernels.cuh"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -63,18 +67,29 @@ def build_duogrid(force: bool = False) -> str:
 def build_bt(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     out = os.path.join(LIBDIR, "libbt.so")
-    srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
+    srcs = [os.path.join(CSRC, s) for s, _ in CUDA_SOURCES]
     deps = srcs + [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [
         os.path.join(INCLUDE, "licom_bt.h"), __file__]
     if force or _newer(out, deps):
-        # -fmad=false: no FMA contraction, so the float64 kernels round like the
-        # reference's float64 NumPy/XLA arithmetic term by term.
-        cmd = [NVCC, *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "-fmad=false", "--shared",
-               "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC, "-lcudart",
-               *srcs, "-o", out + ".tmp"]
-        if verbose_ptxas:
-            cmd.insert(3, "-Xptxas=-v")
-        _run(cmd)
+        objdir = os.path.join(HERE, "_build")
+        os.makedirs(objdir, exist_ok=True)
+        objs = []
+        from concurrent.futures import ThreadPoolExecutor
+
+        def compile_one(item):
+            src, flags = item
+            obj = os.path.join(objdir, os.path.basename(src) + ".o")
+            cmd = [NVCC, *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", *flags,
+                   "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src),
+                   "-o", obj]
+            if verbose_ptxas:
+                cmd.insert(3, "-Xptxas=-v")
+            _run(cmd)
+            return obj
+
+        with ThreadPoolExecutor(max_workers=len(CUDA_SOURCES)) as ex:
+            objs = list(ex.map(compile_one, CUDA_SOURCES))
+        _run([NVCC, *ARCH_FLAGS, "--shared", "-Xcompiler", "-fPIC", *objs, "-lcudart", "-o", out + ".tmp"])
         os.replace(out + ".tmp", out)
     return out
 

@@ -1,4 +1,8 @@
-// bt_kernels.cu - sm_100a kernels of the barotropic duogrid solver and their launchers.
+// bt_kernels.cuh - sm_100a kernels of the barotropic duogrid solver and their launchers.
+//
+// Included by bt_kernels_f64.cu (float64 drop-in, compiled with -fmad=false so
+// the arithmetic rounds like the reference term by term) and bt_kernels_f32.cu
+// (float32 precision form, FMA contraction allowed), each instantiating one type.
 //
 // Per RK stage two tile kernels run back to back (phase H, phase UV); each CTA
 // stages one tile of one face plus its 3-cell stencil halo in shared memory
@@ -8,17 +12,20 @@
 // inside the tile loader (bt_stencil.cuh), so no separate exchange kernel
 // runs between phases.
 
+#pragma once
+
 #include <algorithm>
 
 #include "bt_launch.cuh"
 
 namespace bt {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = kTileThreads;
 
 template <typename T, int TI, int TJ>
 __global__ void __launch_bounds__(kThreads) k_phase_h(Geo<T> g, StageIO<T> io, Tiling t) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  release_dependents();
   const TileBox b = tile_box(t, g.n, blockIdx.x);
   tile_h<T, TI, TJ>(g, io, b, reinterpret_cast<T*>(smraw));
 }
@@ -26,6 +33,7 @@ __global__ void __launch_bounds__(kThreads) k_phase_h(Geo<T> g, StageIO<T> io, T
 template <typename T, int TI, int TJ>
 __global__ void __launch_bounds__(kThreads) k_phase_uv(Geo<T> g, StageIO<T> io, Tiling t) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  release_dependents();
   const TileBox b = tile_box(t, g.n, blockIdx.x);
   tile_uv<T, TI, TJ>(g, io, b, reinterpret_cast<T*>(smraw));
 }
@@ -33,7 +41,7 @@ __global__ void __launch_bounds__(kThreads) k_phase_uv(Geo<T> g, StageIO<T> io, 
 // One whole round of one member in a single cooperative launch: every CTA
 // walks the tiles of a phase, then all CTAs meet at a grid barrier.
 template <typename T, int TI, int TJ>
-__global__ void __launch_bounds__(kThreads) k_round(RoundArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, 2) k_round(RoundArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const int ntiles = 6 * a.t.tiles_per_face();
@@ -58,6 +66,7 @@ __global__ void __launch_bounds__(kThreads) k_round(RoundArgs<T> a) {
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_fill_halo(Geo<T> g, T* h, T* u, T* v) {
+  wait_prior_grid();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < 6 * g.nh) fill_halo_cell(g, h, u, v, k);
 }
@@ -65,6 +74,7 @@ __global__ void __launch_bounds__(kThreads) k_fill_halo(Geo<T> g, T* h, T* u, T*
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_diag(Geo<T> g, const T* h, const T* u, const T* v,
                                                    DiagOut<T> d) {
+  wait_prior_grid();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int m = g.m;
   if (k >= 6 * m * m) return;
@@ -73,6 +83,7 @@ __global__ void __launch_bounds__(kThreads) k_diag(Geo<T> g, const T* h, const T
   diag_cell(g, h, u, v, d, f, r / m, r % m);
 }
 
+#ifdef BT_DEFINE_COMMON
 bool tile_cfg_supported(TileCfg c) {
   return (c.tj == 32 && (c.ti == 4 || c.ti == 8 || c.ti == 16)) ||
          (c.tj == 16 && (c.ti == 8 || c.ti == 16));
@@ -86,6 +97,7 @@ Tiling make_tiling(TileCfg c, int n) {
   t.ntj = (n + c.tj - 1) / c.tj;
   return t;
 }
+#endif
 
 namespace {
 
@@ -134,8 +146,19 @@ cudaError_t launch_tile(const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
   const size_t smem = tile_smem<T, TI, TJ, UV>();
   auto kern = UV ? k_phase_uv<T, TI, TJ> : k_phase_h<T, TI, TJ>;
   const Tiling t = make_tiling({TI, TJ}, g.n);
-  kern<<<6 * t.tiles_per_face(), kThreads, smem, s>>>(g, io, t);
-  return cudaGetLastError();
+  // programmatic dependent launch: the kernel's constant prologue overlaps the
+  // previous kernel's tail; it waits (griddepcontrol.wait) before reading state
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(6 * t.tiles_per_face());
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, g, io, t);
 }
 
 template <typename T, bool UV>
@@ -209,7 +232,5 @@ cudaError_t launch_diag(const Geo<T>& g, const T* h, const T* u, const T* v, con
   template cudaError_t launch_round<T>(const RoundArgs<T>&, TileCfg, int, cudaStream_t, int*);      \
   template cudaError_t launch_diag<T>(const Geo<T>&, const T*, const T*, const T*, const DiagOut<T>&, \
                                       cudaStream_t);
-BT_INSTANTIATE(float)
-BT_INSTANTIATE(double)
 
 }  // namespace bt

@@ -189,13 +189,31 @@ __device__ __forceinline__ int yface_side(int j, int m) {
 // ---------------------------------------------------------------------------
 // Tile phases
 // ---------------------------------------------------------------------------
+// A CTA of kTileThreads threads computes one TI x TJ tile of one face.  Its
+// stencil region (the tile plus 3 cells on each side, without the region
+// corners) is staged into shared memory with cp.async, so every global load
+// of the region is in flight at once; halo cells of the region are gathered
+// (two-level chain: descriptor, then sources), the neighbouring face's edge
+// values are recomputed, and per-cell / per-face constants are prefetched into
+// registers, all before the first barrier.
+constexpr int kTileThreads = 256;
+
 template <int TI, int TJ>
 struct TileShape {
   static constexpr int RI = TI + 6, RJ = TJ + 6, R = RI * RJ;
   static constexpr int FX = (TI + 1) * TJ;   // x faces
   static constexpr int FY = TI * (TJ + 1);   // y faces
-  static constexpr int kWordsH = 3 * R + FX + FY;
-  static constexpr int kWordsUV = 6 * R + 3 * FX + 3 * FY;
+  static constexpr int EW = TI > TJ ? TI : TJ;
+  static constexpr int NE = 4 * EW;          // edge slots: 4 kinds x max(TI, TJ) positions
+  static constexpr int NIT = (R + kTileThreads - 1) / kTileThreads;
+  static constexpr int CIT = (TI * TJ + kTileThreads - 1) / kTileThreads;
+  static constexpr int FIT = (FX + FY + kTileThreads - 1) / kTileThreads;
+  static constexpr int C = TI * TJ;
+  // region: h, u, v, g(4), s, uc, vc [+ hn for UV]; face and cell arrays;
+  // neighbour edge lines (6 contravariant values + 6 h values + depth per slot)
+  static constexpr int kWordsH = 10 * R + 3 * FX + 3 * FY + 2 * C + 13 * NE;
+  static constexpr int kWordsUV = 11 * R + 5 * FX + 5 * FY + 6 * C + 6 * NE;
+  static constexpr int MI = 4;               // gather items per thread handled in the two-sweep path
 };
 
 struct TileBox {
@@ -222,84 +240,437 @@ __device__ __forceinline__ bool region_needed(int r, int c, int ni, int nj) {
   return (rin && c < nj + 6) || (cin && r < ni + 6);
 }
 
+// ---- asynchronous global -> shared copies ---------------------------------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else if (BYTES == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_t(T* dst, const T* src) {
+  cp_async<sizeof(T)>(dst, src);
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_mat(T* dst, const T* src) {  // 4 consecutive T
+  if (sizeof(T) == 8) {
+    cp_async<16>(dst, src);
+    cp_async<16>(dst + 2, src + 2);
+  } else {
+    cp_async<16>(dst, src);
+  }
+}
+
+// ---- halo gathers in two steps (descriptor, then sources) ------------------
+template <typename T>
+struct Pull {
+  int2 s;
+  T w0, w1;
+};
+template <typename T>
+__device__ __forceinline__ Pull<T> pull_desc(const Geo<T>& g, int f, int i, int j) {
+  const int k = f * g.nh + halo_id(i, j, g.m);
+  Pull<T> p;
+  p.s = g.hsrc[k];
+  p.w0 = g.hw[2 * k];
+  p.w1 = g.hw[2 * k + 1];
+  return p;
+}
+template <typename T>
+__device__ __forceinline__ T pull_s(const Pull<T>& p, const T* F) {
+  return p.w0 * F[p.s.x] + p.w1 * F[p.s.y];
+}
+template <typename T>
+__device__ __forceinline__ void pull_v(const Pull<T>& p, const Geo<T>& g, const T* U, const T* V, long o,
+                                       T& u, T& v) {
+  const T* C0 = g.c2l + 4 * (long)p.s.x;
+  const T* C1 = g.c2l + 4 * (long)p.s.y;
+  const T u0 = U[p.s.x], v0 = V[p.s.x], u1 = U[p.s.y], v1 = V[p.s.y];
+  const T ull0 = C0[0] * u0 + C0[1] * v0, vll0 = C0[2] * u0 + C0[3] * v0;
+  const T ull1 = C1[0] * u1 + C1[1] * v1, vll1 = C1[2] * u1 + C1[3] * v1;
+  const T ull = p.w0 * ull0 + p.w1 * ull1;
+  const T vll = p.w0 * vll0 + p.w1 * vll1;
+  const T* L = g.l2c + 4 * o;
+  u = L[0] * ull + L[1] * vll;
+  v = L[2] * ull + L[3] * vll;
+}
+
+// ---- the tile's face-edge positions ----------------------------------------
+// Item q of a tile's edge list: kind 0/1 = x faces of side S/N (position along
+// the tile's columns), kind 2/3 = y faces of side W/E (along the tile's rows).
+struct EdgeItem {
+  int kind, pos, side, k;
+};
+__device__ __forceinline__ int edge_count(const TileBox& b, int m, int* cnt) {
+  cnt[0] = b.i0 == kHalo ? b.nj : 0;
+  cnt[1] = b.i0 + b.ni == m - kHalo ? b.nj : 0;
+  cnt[2] = b.j0 == kHalo ? b.ni : 0;
+  cnt[3] = b.j0 + b.nj == m - kHalo ? b.ni : 0;
+  return cnt[0] + cnt[1] + cnt[2] + cnt[3];
+}
+__device__ __forceinline__ EdgeItem edge_item(const TileBox& b, const int* cnt, int q) {
+  EdgeItem e;
+  int kind = 0;
+  while (q >= cnt[kind]) q -= cnt[kind++];
+  e.kind = kind;
+  e.pos = q;
+  const int sides[4] = {kS, kN, kW, kE};
+  e.side = sides[kind];
+  e.k = kind < 2 ? (b.j0 + q - kHalo) : (b.i0 + q - kHalo);
+  return e;
+}
+
+// Work items of a tile that touches face edges, spread over the whole CTA:
+//   item t < 3P:  halo cell at depth t % 3 outside edge position t / 3 of the
+//                 tile (its h, u, v when the stored halo is not valid, and the
+//                 new h in phase UV) -- a gather from the neighbouring face;
+//   item t >= 3P: point q = (t - 3P) % 6 of the neighbour's 6-point line normal
+//                 to the shared edge at position (t - 3P) / 6: its contravariant
+//                 normal velocity (and h for the mass-flux average).
+// P is the number of edge positions of the tile.  Descriptor loads of all
+// items go out in a first sweep, source loads in a second, so a CTA waits for
+// two L2 round trips instead of one chain per point.
+struct ItemCell {
+  int f, i, j;      // cell whose value the item needs
+  int slot;         // region index (region items) or edge slot*6 + q (line items)
+  int line, y, q;   // line item: 1, normal axis (1 = y), point index
+};
+
+__device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt, int P, int t, int m, int n,
+                                                const int* route, int RJ, int EW) {
+  ItemCell c;
+  if (t < 3 * P) {
+    const EdgeItem e = edge_item(b, cnt, t / 3);
+    const int d = t % 3;
+    int r, cc;
+    switch (e.kind) {
+      case 0: r = d; cc = e.pos + kHalo; break;                  // S: region rows 0..2
+      case 1: r = b.ni + kHalo + d; cc = e.pos + kHalo; break;   // N: rows ni+3..ni+5
+      case 2: r = e.pos + kHalo; cc = d; break;                  // W: region cols 0..2
+      default: r = e.pos + kHalo; cc = b.nj + kHalo + d; break;  // E: cols nj+3..nj+5
+    }
+    c.f = b.f;
+    c.i = b.i0 - kHalo + r;
+    c.j = b.j0 - kHalo + cc;
+    c.slot = r * RJ + cc;
+    c.line = 0;
+    c.y = 0;
+    c.q = 0;
+  } else {
+    const int t2 = t - 3 * P;
+    const EdgeItem e = edge_item(b, cnt, t2 / 6);
+    const int q = t2 % 6;
+    const int r = route[b.f * 4 + e.side];
+    const int ns = route_side(r);
+    const int kk = route_rev(r) ? n - 1 - e.k : e.k;
+    c.f = route_nb(r);
+    edge_point(ns, kk, q, m, c.i, c.j);
+    c.slot = (e.kind * EW + e.pos) * 6 + q;
+    c.line = 1;
+    c.y = (ns == kE || ns == kW);
+    c.q = q;
+  }
+  return c;
+}
+
+template <typename T, int TI, int TJ, bool UV>
+struct Gather {
+  using S = TileShape<TI, TJ>;
+  Pull<T> pd[S::MI];
+  bool pl[S::MI];
+
+  __device__ __forceinline__ static bool needs_pull(const StageIO<T>& io, const ItemCell& c, int m) {
+    return !is_interior(c.i, c.j, m) && (!io.stored_halo || (UV && !c.line));
+  }
+
+  // sweep 1: descriptors of the items' halo gathers (constants, may precede the grid dependency)
+  __device__ __forceinline__ void descriptors(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
+                                              const int* cnt, int P) {
+    const int nitems = 9 * P;
+#pragma unroll
+    for (int k = 0; k < S::MI; ++k) {
+      const int t = threadIdx.x + k * kTileThreads;
+      pl[k] = false;
+      if (t < nitems) {
+        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::RJ, S::EW);
+        if (needs_pull(io, c, g.m)) {
+          pd[k] = pull_desc(g, c.f, c.i, c.j);
+          pl[k] = true;
+        }
+      }
+    }
+  }
+
+  __device__ __forceinline__ void one(const Geo<T>& g, const StageIO<T>& io, const ItemCell& c, const Pull<T>& p,
+                                      bool pull, T* s_h, T* s_u, T* s_v, T* s_hn, T* s_np, T* s_nh, T* s_ndz) {
+    const bool want_h = !UV && io.last;  // neighbour h for the mass-flux average
+    const long o = cell(c.f, c.i, c.j, g.m);
+    if (!c.line) {
+      if (!io.stored_halo) {  // stored halos are staged by cp.async
+        T u, v;
+        pull_v(p, g, io.u, io.v, o, u, v);
+        s_h[c.slot] = pull_s(p, io.h);
+        s_u[c.slot] = u;
+        s_v[c.slot] = v;
+      }
+      if (UV) s_hn[c.slot] = pull_s(p, (const T*)io.h_out);
+    } else {
+      T u, v, h = T(0.0);
+      if (pull) {
+        pull_v(p, g, io.u, io.v, o, u, v);
+        if (want_h) h = pull_s(p, io.h);
+      } else {
+        u = io.u[o];
+        v = io.v[o];
+        if (want_h) h = io.h[o];
+      }
+      s_np[c.slot] = contra(g, o, u, v, c.y);
+      if (want_h) {
+        s_nh[c.slot] = h;
+        if (c.q == 3) s_ndz[c.slot / 6] = c.y ? g.dzph_y[o] : g.dzph_x[o];
+      }
+    }
+  }
+
+  // sweep 2: sources (state, after the grid dependency) and the items' values
+  __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, const int* cnt,
+                                          int P, T* s_h, T* s_u, T* s_v, T* s_hn, T* s_np, T* s_nh, T* s_ndz) {
+    const int nitems = 9 * P;
+#pragma unroll
+    for (int k = 0; k < S::MI; ++k) {
+      const int t = threadIdx.x + k * kTileThreads;
+      if (t < nitems) {
+        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::RJ, S::EW);
+        one(g, io, c, pd[k], pl[k], s_h, s_u, s_v, s_hn, s_np, s_nh, s_ndz);
+      }
+    }
+    // items beyond MI per thread (only tiles spanning several face edges of tiny faces)
+    for (int t = threadIdx.x + S::MI * kTileThreads; t < nitems; t += kTileThreads) {
+      const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::RJ, S::EW);
+      const bool pull = needs_pull(io, c, g.m);
+      Pull<T> p;
+      if (pull) p = pull_desc(g, c.f, c.i, c.j);
+      one(g, io, c, p, pull, s_h, s_u, s_v, s_hn, s_np, s_nh, s_ndz);
+    }
+  }
+};
+
+// Normal velocity of the neighbour's line (6 contravariant values) before averaging.
+template <typename T>
+__device__ __forceinline__ T line_raw(const T* np) {
+  return T(0.5) * (rplus(np, 1) + rminus(np + 1, 1));
+}
+
+// Wait for the previous kernel of the stream (programmatic dependent launch);
+// a no-op when the kernel was launched without a programmatic dependency.
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// Allow the next kernel of the stream to start its prologue.
+__device__ __forceinline__ void release_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+// Constants of the tile's faces and cells, staged by cp.async before the
+// state: depth and c_dy on x faces, depth and d_dx on y faces, and per cell
+// rda (+ rdx, rdy, a_f for phase UV).
+template <typename T, int TI, int TJ, bool UV>
+__device__ __forceinline__ void stage_consts(const Geo<T>& g, const TileBox& b, T* s_dzx, T* s_cdy, T* s_dzy,
+                                             T* s_ddx, T* s_rda, T* s_rdx, T* s_rdy, T* s_af) {
+  using S = TileShape<TI, TJ>;
+  const int m = g.m, f = b.f, tid = threadIdx.x;
+  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
+    if (e < S::FX) {
+      const int a = e / TJ, q = e % TJ;
+      if (a > b.ni || q >= b.nj) continue;
+      const long o = cell(f, b.i0 + a, b.j0 + q, m);
+      cp_async_t(s_dzx + e, g.dzph_x + o);
+      cp_async_t(s_cdy + e, g.c_dy + o);
+    } else {
+      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
+      if (a >= b.ni || q > b.nj) continue;
+      const long o = cell(f, b.i0 + a, b.j0 + q, m);
+      cp_async_t(s_dzy + e2, g.dzph_y + o);
+      cp_async_t(s_ddx + e2, g.d_dx + o);
+    }
+  }
+  for (int e = tid; e < S::C; e += kTileThreads) {
+    const int a = e / TJ, q = e % TJ;
+    if (a >= b.ni || q >= b.nj) continue;
+    const long o = cell(f, b.i0 + a, b.j0 + q, m);
+    cp_async_t(s_rda + e, g.rda + o);
+    if (UV) {
+      cp_async_t(s_rdx + e, g.rdx + o);
+      cp_async_t(s_rdy + e, g.rdy + o);
+      cp_async_t(s_af + e, g.a_f + o);
+    }
+  }
+}
+
+// gct and sina of the region (constants).
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void stage_region_consts(const Geo<T>& g, const TileBox& b, T* s_g, T* s_s) {
+  using S = TileShape<TI, TJ>;
+  constexpr int RJ = S::RJ;
+#pragma unroll
+  for (int it = 0; it < S::NIT; ++it) {
+    const int e = threadIdx.x + it * kTileThreads;
+    if (e >= S::R) break;
+    const int r = e / RJ, c = e - r * RJ;
+    if (!region_needed(r, c, b.ni, b.nj)) continue;
+    const long o = cell(b.f, b.i0 - kHalo + r, b.j0 - kHalo + c, g.m);
+    cp_async_mat(s_g + 4 * e, g.gct + 4 * o);
+    cp_async_t(s_s + e, g.sina + o);
+  }
+}
+
+// State of the region: h, u, v (interior cells, or every cell when the stored
+// halo is valid) and the new h of interior cells when HN.
+template <typename T, int TI, int TJ, bool HN>
+__device__ __forceinline__ void stage_region_state(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
+                                                   T* s_h, T* s_u, T* s_v, T* s_hn) {
+  using S = TileShape<TI, TJ>;
+  constexpr int RJ = S::RJ;
+  const int m = g.m;
+  const T* hn_src = (const T*)io.h_out;
+#pragma unroll
+  for (int it = 0; it < S::NIT; ++it) {
+    const int e = threadIdx.x + it * kTileThreads;
+    if (e >= S::R) break;
+    const int r = e / RJ, c = e - r * RJ;
+    if (!region_needed(r, c, b.ni, b.nj)) continue;
+    const int i = b.i0 - kHalo + r, j = b.j0 - kHalo + c;
+    const long o = cell(b.f, i, j, m);
+    const bool inner = is_interior(i, j, m);
+    if (io.stored_halo || inner) {
+      cp_async_t(s_h + e, io.h + o);
+      cp_async_t(s_u + e, io.u + o);
+      cp_async_t(s_v + e, io.v + o);
+    }
+    if (HN && inner) cp_async_t(s_hn + e, hn_src + o);
+  }
+}
+
 // Phase H of one tile: writes the new h on the tile's interior cells.
 template <typename T, int TI, int TJ>
 __device__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
-  const int m = g.m, f = b.f;
+  const int m = g.m, f = b.f, tid = threadIdx.x;
   T* s_h = sm;
-  T* s_uc = s_h + S::R;
+  T* s_u = s_h + S::R;
+  T* s_v = s_u + S::R;
+  T* s_g = s_v + S::R;      // [R][4]
+  T* s_s = s_g + 4 * S::R;
+  T* s_uc = s_s + S::R;
   T* s_vc = s_uc + S::R;
-  T* s_fu = s_vc + S::R;  // [TI+1][TJ]
-  T* s_fv = s_fu + S::FX; // [TI][TJ+1]
+  T* s_fu = s_vc + S::R;    // [TI+1][TJ] mass flux on x faces
+  T* s_fv = s_fu + S::FX;   // [TI][TJ+1] on y faces
+  T* s_dzx = s_fv + S::FY;  // [TI+1][TJ]
+  T* s_cdy = s_dzx + S::FX;
+  T* s_dzy = s_cdy + S::FX; // [TI][TJ+1]
+  T* s_ddx = s_dzy + S::FY;
+  T* s_rda = s_ddx + S::FY; // [TI][TJ]
+  T* s_hp = s_rda + S::C;
+  T* s_np = s_hp + S::C;    // [NE][6] neighbour line: contravariant normal velocity
+  T* s_nh = s_np + 6 * S::NE;   // [NE][6] neighbour line: h
+  T* s_ndz = s_nh + 6 * S::NE;  // [NE] neighbour depth at the edge face
 
-  for (int e = threadIdx.x; e < S::R; e += blockDim.x) {
+  // constants first: they do not depend on the previous kernel
+  stage_region_consts<T, TI, TJ>(g, b, s_g, s_s);
+  stage_consts<T, TI, TJ, false>(g, b, s_dzx, s_cdy, s_dzy, s_ddx, s_rda, nullptr, nullptr, nullptr);
+  int cnt[4];
+  const int P = edge_count(b, m, cnt);
+  Gather<T, TI, TJ, false> gat;
+  if (P > 0) gat.descriptors(g, io, b, cnt, P);
+  wait_prior_grid();
+  stage_region_state<T, TI, TJ, false>(g, io, b, s_h, s_u, s_v, nullptr);
+  for (int e = tid; e < S::C; e += kTileThreads) {
+    const int a = e / TJ, q = e % TJ;
+    if (a < b.ni && q < b.nj) cp_async_t(s_hp + e, io.hp + cell(f, b.i0 + a, b.j0 + q, m));
+  }
+  if (P > 0) gat.sources(g, io, b, cnt, P, s_h, s_u, s_v, nullptr, s_np, s_nh, s_ndz);
+  cp_async_wait_all();
+  __syncthreads();
+
+  // contravariant velocities on the region (remap.py:34-39)
+#pragma unroll
+  for (int it = 0; it < S::NIT; ++it) {
+    const int e = tid + it * kTileThreads;
+    if (e >= S::R) break;
     const int r = e / RJ, c = e - r * RJ;
     if (!region_needed(r, c, b.ni, b.nj)) continue;
-    const int i = b.i0 - kHalo + r, j = b.j0 - kHalo + c;
-    const long o = cell(f, i, j, m);
-    T u, v;
-    fetch_v(io.u, io.v, g, f, i, j, io.stored_halo, u, v);
-    s_h[e] = fetch_s(io.h, g, f, i, j, io.stored_halo);
-    s_uc[e] = contra(g, o, u, v, 0);
-    s_vc[e] = contra(g, o, u, v, 1);
+    const T* G = s_g + 4 * e;
+    const T u = s_u[e], v = s_v[e], sn = s_s[e];
+    s_uc[e] = (G[0] * u + G[1] * v) * sn;
+    s_vc[e] = (G[2] * u + G[3] * v) * sn;
   }
   __syncthreads();
 
-  // x faces i = i0 .. i0+ni, columns of the tile
-  for (int e = threadIdx.x; e < (b.ni + 1) * b.nj; e += blockDim.x) {
-    const int a = e / b.nj, q = e - a * b.nj;
-    const int i = b.i0 + a, j = b.j0 + q;
-    const int base = a * RJ + (q + kHalo);  // local (row of cell i) - 3
+  // faces: x faces i = i0..i0+ni on the tile's columns, then y faces j = j0..j0+nj on its rows
+  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
+    const bool xf = e < S::FX;
+    int a, q, stride, base, side, kind, pos, fi;
+    if (xf) {
+      a = e / TJ;
+      q = e % TJ;
+      if (a > b.ni || q >= b.nj) continue;
+      stride = RJ;
+      base = a * RJ + (q + kHalo);
+      side = xface_side(b.i0 + a, m);
+      kind = side == kS ? 0 : 1;
+      pos = q;
+      fi = e;
+    } else {
+      fi = e - S::FX;
+      a = fi / (TJ + 1);
+      q = fi % (TJ + 1);
+      if (a >= b.ni || q > b.nj) continue;
+      stride = 1;
+      base = (a + kHalo) * RJ + q;
+      side = yface_side(b.j0 + q, m);
+      kind = side == kW ? 2 : 3;
+      pos = a;
+    }
     const T* ph = s_h + base;
-    const T* pu = s_uc + base;
-    const T ue = rplus(pu, RJ), uw = rminus(pu + RJ, RJ);
+    const T* pu = (xf ? s_uc : s_vc) + base;
+    const T ue = rplus(pu, stride), uw = rminus(pu + stride, stride);
     T bc = T(0.5) * (ue + uw);
-    const int side = xface_side(i, m);
-    if (side >= 0) bc = (bc + nb_normal_raw(g, io.u, io.v, io.stored_halo, f, side, j - kHalo)) / T(2.0);
-    const long o = cell(f, i, j, m);
-    const T dz = g.dzph_x[o];
-    const T he = rplus(ph, RJ), hw = rminus(ph + RJ, RJ);
-    const T cx = celerity(mid6(ph, RJ), dz);
-    const T vis = bc + (T(4.9) / cx) * (he - hw);
-    T fu = dz * vis + (vis > T(0.0) ? he : hw) * vis;
-    if (io.last && side >= 0)
-      fu = (fu + nb_mass_flux(g, io.h, io.stored_halo, f, side, j - kHalo, bc)) / T(2.0);
-    s_fu[a * TJ + q] = fu;
-  }
-  // y faces j = j0 .. j0+nj, rows of the tile
-  for (int e = threadIdx.x; e < b.ni * (b.nj + 1); e += blockDim.x) {
-    const int a = e / (b.nj + 1), q = e - a * (b.nj + 1);
-    const int i = b.i0 + a, j = b.j0 + q;
-    const int base = (a + kHalo) * RJ + q;
-    const T* ph = s_h + base;
-    const T* pv = s_vc + base;
-    const T vn = rplus(pv, 1), vs = rminus(pv + 1, 1);
-    T bc = T(0.5) * (vn + vs);
-    const int side = yface_side(j, m);
-    if (side >= 0) bc = (bc + nb_normal_raw(g, io.u, io.v, io.stored_halo, f, side, i - kHalo)) / T(2.0);
-    const long o = cell(f, i, j, m);
-    const T dz = g.dzph_y[o];
-    const T hn = rplus(ph, 1), hs = rminus(ph + 1, 1);
-    const T cy = celerity(mid6(ph, 1), dz);
-    const T vis = bc + (T(4.9) / cy) * (hn - hs);
-    T fv = dz * vis + (vis > T(0.0) ? hn : hs) * vis;
-    if (io.last && side >= 0)
-      fv = (fv + nb_mass_flux(g, io.h, io.stored_halo, f, side, i - kHalo, bc)) / T(2.0);
-    s_fv[a * (TJ + 1) + q] = fv;
+    const int slot = kind * S::EW + pos;
+    if (side >= 0) bc = (bc + line_raw(s_np + 6 * slot)) / T(2.0);
+    const T dz = xf ? s_dzx[fi] : s_dzy[fi];
+    const T he = rplus(ph, stride), hw = rminus(ph + stride, stride);
+    const T cc = celerity(mid6(ph, stride), dz);
+    const T vis = bc + (T(4.9) / cc) * (he - hw);
+    T fl = dz * vis + (vis > T(0.0) ? he : hw) * vis;
+    if (io.last && side >= 0) {  // the neighbour's flux at the same edge face (barotr_pure.py:29-49)
+      const T* nh = s_nh + 6 * slot;
+      const T ndz = s_ndz[slot];
+      const T nhe = rplus(nh, 1), nhw = rminus(nh + 1, 1);
+      const T nc = celerity(mid6(nh, 1), ndz);
+      const T nvis = bc + (T(4.9) / nc) * (nhe - nhw);
+      fl = (fl + (ndz * nvis + (nvis > T(0.0) ? nhe : nhw) * nvis)) / T(2.0);
+    }
+    if (xf)
+      s_fu[fi] = fl;
+    else
+      s_fv[fi] = fl;
   }
   __syncthreads();
 
   // cells: divergence (agrid.py:43-53) and the h update (barotr_pure.py:119-120)
-  for (int e = threadIdx.x; e < b.ni * b.nj; e += blockDim.x) {
-    const int a = e / b.nj, q = e - a * b.nj;
-    const int i = b.i0 + a, j = b.j0 + q;
-    const long o = cell(f, i, j, m);
-    const T fu0 = s_fu[a * TJ + q], fu1 = s_fu[(a + 1) * TJ + q];
-    const T fv0 = s_fv[a * (TJ + 1) + q], fv1 = s_fv[a * (TJ + 1) + q + 1];
-    const T div = g.rda[o] * (fu1 * g.c_dy[o + m] - fu0 * g.c_dy[o] + fv1 * g.d_dx[o + 1] - fv0 * g.d_dx[o]);
-    io.h_out[o] = io.hp[o] - div * io.dt;
+  for (int e = tid; e < S::C; e += kTileThreads) {
+    const int a = e / TJ, q = e % TJ;
+    if (a >= b.ni || q >= b.nj) continue;
+    const long o = cell(f, b.i0 + a, b.j0 + q, m);
+    const int x0 = e, x1 = e + TJ;
+    const int y0 = a * (TJ + 1) + q, y1 = y0 + 1;
+    const T div = s_rda[x0] * (s_fu[x1] * s_cdy[x1] - s_fu[x0] * s_cdy[x0] + s_fv[y1] * s_ddx[y1] -
+                               s_fv[y0] * s_ddx[y0]);
+    io.h_out[o] = s_hp[x0] - div * io.dt;
   }
 }
 
@@ -309,106 +680,139 @@ template <typename T, int TI, int TJ>
 __device__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
-  const int m = g.m, f = b.f;
+  const int m = g.m, f = b.f, tid = threadIdx.x;
   T* s_h = sm;
-  T* s_uc = s_h + S::R;
-  T* s_vc = s_uc + S::R;
-  T* s_u = s_vc + S::R;
+  T* s_u = s_h + S::R;
   T* s_v = s_u + S::R;
-  T* s_hb = s_v + S::R;
-  T* s_ku = s_hb + S::R;   // x faces [TI+1][TJ]: kinetic energy, tangential v, viscous flux
+  T* s_g = s_v + S::R;      // [R][4]
+  T* s_s = s_g + 4 * S::R;
+  T* s_uc = s_s + S::R;
+  T* s_vc = s_uc + S::R;
+  T* s_hn = s_vc + S::R;    // new h, then the blended h of the pressure gradient
+  T* s_ku = s_hn + S::R;    // x faces [TI+1][TJ]: kinetic energy, tangential v, viscous flux
   T* s_vx = s_ku + S::FX;
   T* s_fx = s_vx + S::FX;
-  T* s_kv = s_fx + S::FX;  // y faces [TI][TJ+1]
+  T* s_dzx = s_fx + S::FX;
+  T* s_cdy = s_dzx + S::FX;
+  T* s_kv = s_cdy + S::FX;  // y faces [TI][TJ+1]
   T* s_uy = s_kv + S::FY;
   T* s_fy = s_uy + S::FY;
+  T* s_dzy = s_fy + S::FY;
+  T* s_ddx = s_dzy + S::FY;
+  T* s_rda = s_ddx + S::FY; // cells [TI][TJ]
+  T* s_rdx = s_rda + S::C;
+  T* s_rdy = s_rdx + S::C;
+  T* s_af = s_rdy + S::C;
+  T* s_up = s_af + S::C;
+  T* s_vp = s_up + S::C;
+  T* s_np = s_vp + S::C;    // [NE][6] neighbour line: contravariant normal velocity
 
-  for (int e = threadIdx.x; e < S::R; e += blockDim.x) {
+  stage_region_consts<T, TI, TJ>(g, b, s_g, s_s);
+  stage_consts<T, TI, TJ, true>(g, b, s_dzx, s_cdy, s_dzy, s_ddx, s_rda, s_rdx, s_rdy, s_af);
+  int cnt[4];
+  const int P = edge_count(b, m, cnt);
+  Gather<T, TI, TJ, true> gat;
+  if (P > 0) gat.descriptors(g, io, b, cnt, P);
+  wait_prior_grid();
+  stage_region_state<T, TI, TJ, true>(g, io, b, s_h, s_u, s_v, s_hn);
+  for (int e = tid; e < S::C; e += kTileThreads) {
+    const int a = e / TJ, q = e % TJ;
+    if (a >= b.ni || q >= b.nj) continue;
+    const long o = cell(f, b.i0 + a, b.j0 + q, m);
+    cp_async_t(s_up + e, io.up + o);
+    cp_async_t(s_vp + e, io.vp + o);
+  }
+  if (P > 0) gat.sources(g, io, b, cnt, P, s_h, s_u, s_v, s_hn, s_np, nullptr, nullptr);
+  cp_async_wait_all();
+  __syncthreads();
+
+#pragma unroll
+  for (int it = 0; it < S::NIT; ++it) {
+    const int e = tid + it * kTileThreads;
+    if (e >= S::R) break;
     const int r = e / RJ, c = e - r * RJ;
     if (!region_needed(r, c, b.ni, b.nj)) continue;
-    const int i = b.i0 - kHalo + r, j = b.j0 - kHalo + c;
-    const long o = cell(f, i, j, m);
-    T u, v;
-    fetch_v(io.u, io.v, g, f, i, j, io.stored_halo, u, v);
-    const T h = fetch_s(io.h, g, f, i, j, io.stored_halo);
-    const T hn = fetch_s((const T*)io.h_out, g, f, i, j, 0);
-    s_h[e] = h;
-    s_u[e] = u;
-    s_v[e] = v;
-    s_uc[e] = contra(g, o, u, v, 0);
-    s_vc[e] = contra(g, o, u, v, 1);
-    s_hb[e] = (T(1.0) - io.beta) * hn + io.beta * h;  // fb_scheme, barotr_pure.py:52-54
+    const T* G = s_g + 4 * e;
+    const T u = s_u[e], v = s_v[e], sn = s_s[e];
+    s_uc[e] = (G[0] * u + G[1] * v) * sn;
+    s_vc[e] = (G[2] * u + G[3] * v) * sn;
+    s_hn[e] = (T(1.0) - io.beta) * s_hn[e] + io.beta * s_h[e];  // fb_scheme, barotr_pure.py:52-54
   }
   __syncthreads();
 
-  // x faces
-  for (int e = threadIdx.x; e < (b.ni + 1) * b.nj; e += blockDim.x) {
-    const int a = e / b.nj, q = e - a * b.nj;
-    const int i = b.i0 + a, j = b.j0 + q;
-    const int base = a * RJ + (q + kHalo);
+  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
+    const bool xf = e < S::FX;
+    int a, q, stride, base, side, kind, pos, fi;
+    if (xf) {
+      a = e / TJ;
+      q = e % TJ;
+      if (a > b.ni || q >= b.nj) continue;
+      stride = RJ;
+      base = a * RJ + (q + kHalo);
+      side = xface_side(b.i0 + a, m);
+      kind = side == kS ? 0 : 1;
+      pos = q;
+      fi = e;
+    } else {
+      fi = e - S::FX;
+      a = fi / (TJ + 1);
+      q = fi % (TJ + 1);
+      if (a >= b.ni || q > b.nj) continue;
+      stride = 1;
+      base = (a + kHalo) * RJ + q;
+      side = yface_side(b.j0 + q, m);
+      kind = side == kW ? 2 : 3;
+      pos = a;
+    }
     const T* ph = s_h + base;
-    const T* pu = s_uc + base;
-    const T* pv = s_v + base;
-    const T ue = rplus(pu, RJ), uw = rminus(pu + RJ, RJ);
+    const T* pn = (xf ? s_uc : s_vc) + base;   // normal contravariant component
+    const T* pt = (xf ? s_v : s_u) + base;     // raw tangential component (remap.py:84-94)
+    const T ue = rplus(pn, stride), uw = rminus(pn + stride, stride);
     T bc = T(0.5) * (ue + uw);
-    const int side = xface_side(i, m);
-    if (side >= 0) bc = (bc + nb_normal_raw(g, io.u, io.v, io.stored_halo, f, side, j - kHalo)) / T(2.0);
-    const T vt = bc > T(0.0) ? rplus(pv, RJ) : rminus(pv + RJ, RJ);   // remap.py:84-88
-    const long o = cell(f, i, j, m);
-    const T cx = celerity(mid6(ph, RJ), g.dzph_x[o]);
-    const T vis = bc + (T(4.9) / cx) * (rplus(ph, RJ) - rminus(ph + RJ, RJ));
-    s_ku[a * TJ + q] = T(0.5) * (vis * vis + vt * vt);
-    s_vx[a * TJ + q] = vt;
-    s_fx[a * TJ + q] = T(0.5) * cx * (ue - uw);                       // barotr_pure.py:68
-  }
-  // y faces
-  for (int e = threadIdx.x; e < b.ni * (b.nj + 1); e += blockDim.x) {
-    const int a = e / (b.nj + 1), q = e - a * (b.nj + 1);
-    const int i = b.i0 + a, j = b.j0 + q;
-    const int base = (a + kHalo) * RJ + q;
-    const T* ph = s_h + base;
-    const T* pv = s_vc + base;
-    const T* pu = s_u + base;
-    const T vn = rplus(pv, 1), vs = rminus(pv + 1, 1);
-    T bc = T(0.5) * (vn + vs);
-    const int side = yface_side(j, m);
-    if (side >= 0) bc = (bc + nb_normal_raw(g, io.u, io.v, io.stored_halo, f, side, i - kHalo)) / T(2.0);
-    const T ut = bc > T(0.0) ? rplus(pu, 1) : rminus(pu + 1, 1);       // remap.py:90-94
-    const long o = cell(f, i, j, m);
-    const T cy = celerity(mid6(ph, 1), g.dzph_y[o]);
-    const T vis = bc + (T(4.9) / cy) * (rplus(ph, 1) - rminus(ph + 1, 1));
-    s_kv[a * (TJ + 1) + q] = T(0.5) * (vis * vis + ut * ut);
-    s_uy[a * (TJ + 1) + q] = ut;
-    s_fy[a * (TJ + 1) + q] = T(0.5) * cy * (vn - vs);                  // barotr_pure.py:69
+    if (side >= 0) bc = (bc + line_raw(s_np + 6 * (kind * S::EW + pos))) / T(2.0);
+    const T vt = bc > T(0.0) ? rplus(pt, stride) : rminus(pt + stride, stride);
+    const T cc = celerity(mid6(ph, stride), xf ? s_dzx[fi] : s_dzy[fi]);
+    const T vis = bc + (T(4.9) / cc) * (rplus(ph, stride) - rminus(ph + stride, stride));
+    const T kin = T(0.5) * (vis * vis + vt * vt);
+    const T fvis = T(0.5) * cc * (ue - uw);   // barotr_pure.py:68-69
+    if (xf) {
+      s_ku[fi] = kin;
+      s_vx[fi] = vt;
+      s_fx[fi] = fvis;
+    } else {
+      s_kv[fi] = kin;
+      s_uy[fi] = vt;
+      s_fy[fi] = fvis;
+    }
   }
   __syncthreads();
 
-  for (int e = threadIdx.x; e < b.ni * b.nj; e += blockDim.x) {
-    const int a = e / b.nj, q = e - a * b.nj;
-    const int i = b.i0 + a, j = b.j0 + q;
-    const long o = cell(f, i, j, m);
-    const int xf0 = a * TJ + q, xf1 = (a + 1) * TJ + q;
+  for (int e = tid; e < S::C; e += kTileThreads) {
+    const int a = e / TJ, q = e % TJ;
+    if (a >= b.ni || q >= b.nj) continue;
+    const long o = cell(f, b.i0 + a, b.j0 + q, m);
+    const int xf0 = e, xf1 = e + TJ;
     const int yf0 = a * (TJ + 1) + q, yf1 = yf0 + 1;
     const int lc = (a + kHalo) * RJ + (q + kHalo);
     const T uct = s_uc[lc], vct = s_vc[lc];
-    const T rdx = g.rdx[o], rdy = g.rdy[o];
+    const T rdx = s_rdx[xf0], rdy = s_rdy[xf0];
     // vorticity (agrid.py:31-41) and advection (barotr_pure.py:78-97)
-    const T vort = g.rda[o] * (s_uy[yf0] * g.d_dx[o] + s_vx[xf1] * g.c_dy[o + m] -
-                               s_uy[yf1] * g.d_dx[o + 1] - s_vx[xf0] * g.c_dy[o]);
+    const T vort = s_rda[xf0] * (s_uy[yf0] * s_ddx[yf0] + s_vx[xf1] * s_cdy[xf1] - s_uy[yf1] * s_ddx[yf1] -
+                                 s_vx[xf0] * s_cdy[xf0]);
     const T advx = vort * vct - (s_ku[xf1] - s_ku[xf0]) * rdx;
     const T advy = -vort * uct - (s_kv[yf1] - s_kv[yf0]) * rdy;
     // celerity viscosity (barotr_pure.py:63-75)
     const T visx = -(rdx * (s_fx[xf1] - s_fx[xf0]));
     const T visy = -(rdy * (s_fy[yf1] - s_fy[yf0]));
     // pressure gradient of the new h (agrid.py:55-69, barotr_pure.py:57-60)
-    const T* pbx = s_hb + (a * RJ + (q + kHalo));
-    const T* pby = s_hb + ((a + kHalo) * RJ + q);
+    const T* pbx = s_hn + (a * RJ + (q + kHalo));
+    const T* pby = s_hn + ((a + kHalo) * RJ + q);
     const T pgu = T(-9.80) * (rdx * (mid6(pbx + RJ, RJ) - mid6(pbx, RJ)));
     const T pgv = T(-9.80) * (rdy * (mid6(pby + 1, 1) - mid6(pby, 1)));
-    const T af = g.a_f[o];
+    const T af = s_af[xf0];
     // momentum update (barotr_pure.py:149-150)
-    io.u_out[o] = io.up[o] + (pgu + advx + af * vct + visx) * io.dt;
-    io.v_out[o] = io.vp[o] + (pgv + advy - af * uct + visy) * io.dt;
+    io.u_out[o] = s_up[xf0] + (pgu + advx + af * vct + visx) * io.dt;
+    io.v_out[o] = s_vp[xf0] + (pgv + advy - af * uct + visy) * io.dt;
   }
 }
 
