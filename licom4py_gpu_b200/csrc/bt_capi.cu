@@ -106,8 +106,13 @@ struct bt_plan {
   size_t tev_used = 0;
 
   size_t esize() const { return dtype == BT_F64 ? 8 : 4; }
+  // scratch layout: 6 stage fields, edge lines (24 n), face caches x and y (6 (n+1) n 3 each)
+  size_t face_elems() const { return (size_t)6 * (n + 1) * n * 3; }
+  size_t scratch_elems() const { return 6 * field_elems + 24 * (size_t)n + 2 * face_elems(); }
   void* scratch_field(int k) const { return (char*)scratch + (size_t)k * field_elems * esize(); }
   void* edge_lines() const { return scratch_field(6); }
+  void* face_x() const { return (char*)edge_lines() + 24 * (size_t)n * esize(); }
+  void* face_y() const { return (char*)face_x() + face_elems() * esize(); }
 
   template <typename T>
   Geo<T> geo() const {
@@ -230,9 +235,11 @@ int build_tables(bt_plan* p, const bt_grid_desc* d) {
 }
 
 template <typename T>
-StageIO<T> stage_io(const T* h, const T* u, const T* v, const T* hp, const T* up, const T* vp, T* ho, T* uo,
-                    T* vo, double dt, double beta, int stored, int last) {
+StageIO<T> stage_io(const bt_plan* p, const T* h, const T* u, const T* v, const T* hp, const T* up, const T* vp,
+                    T* ho, T* uo, T* vo, double dt, double beta, int stored, int last) {
   StageIO<T> io;
+  io.fx = (T*)p->face_x();
+  io.fy = (T*)p->face_y();
   io.h = h;
   io.u = u;
   io.v = v;
@@ -273,20 +280,20 @@ cudaError_t enqueue_round(const bt_plan* p, const bt_state_in& in, const bt_stat
     const int stored = step == 0 ? 1 : 0;
     if (rk == 2) {
       // barotr.py:50-56: dt/2 from the base, then dt from the same base
-      e = run_stage<T>(p, g, stage_io<T>(cur[0], cur[1], cur[2], base[0], base[1], base[2], Y[0], Y[1], Y[2],
+      e = run_stage<T>(p, g, stage_io<T>(p, cur[0], cur[1], cur[2], base[0], base[1], base[2], Y[0], Y[1], Y[2],
                                          dtb / 2.0, 0.0, stored, 0), s);
       if (e != cudaSuccess) return e;
-      e = run_stage<T>(p, g, stage_io<T>(Y[0], Y[1], Y[2], base[0], base[1], base[2], X[0], X[1], X[2], dtb,
+      e = run_stage<T>(p, g, stage_io<T>(p, Y[0], Y[1], Y[2], base[0], base[1], base[2], X[0], X[1], X[2], dtb,
                                          0.0, 0, 1), s);
     } else {
       // barotr.py:73-83: dt/3, dt/2, dt with beta_d = 1
-      e = run_stage<T>(p, g, stage_io<T>(cur[0], cur[1], cur[2], base[0], base[1], base[2], Y[0], Y[1], Y[2],
+      e = run_stage<T>(p, g, stage_io<T>(p, cur[0], cur[1], cur[2], base[0], base[1], base[2], Y[0], Y[1], Y[2],
                                          dtb / 3.0, 1.0, stored, 0), s);
       if (e != cudaSuccess) return e;
-      e = run_stage<T>(p, g, stage_io<T>(Y[0], Y[1], Y[2], base[0], base[1], base[2], Z[0], Z[1], Z[2],
+      e = run_stage<T>(p, g, stage_io<T>(p, Y[0], Y[1], Y[2], base[0], base[1], base[2], Z[0], Z[1], Z[2],
                                          dtb / 2.0, 1.0, 0, 0), s);
       if (e != cudaSuccess) return e;
-      e = run_stage<T>(p, g, stage_io<T>(Z[0], Z[1], Z[2], base[0], base[1], base[2], X[0], X[1], X[2], dtb,
+      e = run_stage<T>(p, g, stage_io<T>(p, Z[0], Z[1], Z[2], base[0], base[1], base[2], X[0], X[1], X[2], dtb,
                                          1.0, 0, 1), s);
     }
     if (e != cudaSuccess) return e;
@@ -309,7 +316,7 @@ cudaError_t enqueue_stage(const bt_plan* p, const bt_state_in& in, const bt_stat
                           double beta, int last, cudaStream_t s) {
   const Geo<T> g = p->geo<T>();
   T* X[3] = {(T*)out.h0, (T*)out.ub, (T*)out.vb};
-  const StageIO<T> io = stage_io<T>((const T*)in.h0, (const T*)in.ub, (const T*)in.vb, (const T*)in.h0p,
+  const StageIO<T> io = stage_io<T>(p, (const T*)in.h0, (const T*)in.ub, (const T*)in.vb, (const T*)in.h0p,
                                     (const T*)in.ubp, (const T*)in.vbp, X[0], X[1], X[2], dt, beta, 1, last);
   cudaError_t e = run_stage<T>(p, g, io, s);
   if (e != cudaSuccess) return e;
@@ -342,6 +349,8 @@ cudaError_t enqueue_round_persistent(bt_plan* p, const bt_state_in& in, const bt
   a.x[0] = (T*)out.h0;
   a.x[1] = (T*)out.ub;
   a.x[2] = (T*)out.vb;
+  a.fx = (T*)p->face_x();
+  a.fy = (T*)p->face_y();
   a.nbb = nbb;
   a.rk = rk;
   a.dtb = dtb;
@@ -472,7 +481,7 @@ int bt_plan_create(const bt_grid_desc* d, bt_plan** out) {
     bt_plan_destroy(p);
     return rc;
   }
-  const size_t bytes = (6 * p->field_elems + 24 * (size_t)p->n) * p->esize();
+  const size_t bytes = p->scratch_elems() * p->esize();
   cudaError_t e = cudaMalloc(&p->scratch, bytes);
   if (e != cudaSuccess) {
     bt_plan_destroy(p);
@@ -684,7 +693,7 @@ long long bt_plan_get_info(bt_plan* p, int key) {
   if (!p) return -1;
   switch (key) {
     case BT_INFO_LAST_GRID: return p->last_grid;
-    case BT_INFO_SCRATCH_BYTES: return (long long)((6 * p->field_elems + 24 * (size_t)p->n) * p->esize());
+    case BT_INFO_SCRATCH_BYTES: return (long long)(p->scratch_elems() * p->esize());
     default: return -1;
   }
 }

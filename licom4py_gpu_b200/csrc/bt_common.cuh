@@ -86,6 +86,8 @@ struct StageIO {
   T* h_out;     // stage outputs (interior cells only)
   T* u_out;
   T* v_out;
+  T* fx;        // face cache, x faces (6, N+1, N, 3): averaged normal velocity,
+  T* fy;        // its viscous correction, celerity flux; y faces (6, N, N+1, 3)
   T dt;
   T beta;
   int stored_halo;  // 1: the inputs' halo cells hold valid values (first stage of a round)
@@ -115,6 +117,8 @@ struct RoundArgs {
   T* x[3];         // output / running state
   T* y[3];         // stage scratch
   T* z[3];         // second stage scratch (RK3)
+  T* fx;           // face caches (phase H -> phase UV)
+  T* fy;
   int nbb, rk;
   double dtb;
   unsigned* bar;   // grid barrier counter, zero at launch

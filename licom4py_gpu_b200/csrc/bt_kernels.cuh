@@ -107,6 +107,12 @@ size_t tile_smem() {
   return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH);
 }
 
+// The persistent kernel runs both phases in one allocation: the larger of the two.
+template <typename T, int TI, int TJ>
+size_t round_smem() {
+  return std::max(tile_smem<T, TI, TJ, false>(), tile_smem<T, TI, TJ, true>());
+}
+
 // Opt in to more than 48 KB of dynamic shared memory (done at plan creation,
 // never during stream capture).
 template <typename T, int TI, int TJ>
@@ -115,7 +121,7 @@ cudaError_t prime_tile() {
                                        (int)tile_smem<T, TI, TJ, false>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_round<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)tile_smem<T, TI, TJ, true>());
+                           (int)round_smem<T, TI, TJ>());
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_phase_uv<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)tile_smem<T, TI, TJ, true>());
@@ -124,7 +130,7 @@ cudaError_t prime_tile() {
 // Co-resident grid for the persistent kernel (at most one CTA per tile).
 template <typename T, int TI, int TJ>
 cudaError_t launch_round_tile(RoundArgs<T> a, int max_ctas, cudaStream_t s, int* grid_out) {
-  const size_t smem = tile_smem<T, TI, TJ, true>();
+  const size_t smem = round_smem<T, TI, TJ>();
   int dev, sms, per_sm;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;

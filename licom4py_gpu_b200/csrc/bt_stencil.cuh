@@ -212,7 +212,9 @@ struct TileShape {
   // region: h, u, v, g(4), s, uc, vc [+ hn for UV]; face and cell arrays;
   // neighbour edge lines (6 contravariant values + 6 h values + depth per slot)
   static constexpr int kWordsH = 10 * R + 3 * FX + 3 * FY + 2 * C + 13 * NE;
-  static constexpr int kWordsUV = 11 * R + 5 * FX + 5 * FY + 6 * C + 6 * NE;
+  // UV: cells g(4), s, rda, rdx, rdy, af, up, vp; region u, v, hn, h; faces:
+  // cache (3) + kinetic energy + tangential + c_dy / d_dx
+  static constexpr int kWordsUV = 11 * C + 4 * R + 6 * FX + 6 * FY;
   static constexpr int MI = 4;               // gather items per thread handled in the two-sweep path
 };
 
@@ -383,6 +385,9 @@ __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt
 template <typename T, int TI, int TJ, bool UV>
 struct Gather {
   using S = TileShape<TI, TJ>;
+  // phase H gathers the region halo and the neighbour edge lines (9 items per
+  // edge position); phase UV only the region halo (3 per position)
+  static constexpr int kPerPos = UV ? 3 : 9;
   Pull<T> pd[S::MI];
   bool pl[S::MI];
 
@@ -393,7 +398,7 @@ struct Gather {
   // sweep 1: descriptors of the items' halo gathers (constants, may precede the grid dependency)
   __device__ __forceinline__ void descriptors(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
                                               const int* cnt, int P) {
-    const int nitems = 9 * P;
+    const int nitems = kPerPos * P;
 #pragma unroll
     for (int k = 0; k < S::MI; ++k) {
       const int t = threadIdx.x + k * kTileThreads;
@@ -442,7 +447,7 @@ struct Gather {
   // sweep 2: sources (state, after the grid dependency) and the items' values
   __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, const int* cnt,
                                           int P, T* s_h, T* s_u, T* s_v, T* s_hn, T* s_np, T* s_nh, T* s_ndz) {
-    const int nitems = 9 * P;
+    const int nitems = kPerPos * P;
 #pragma unroll
     for (int k = 0; k < S::MI; ++k) {
       const int t = threadIdx.x + k * kTileThreads;
@@ -654,10 +659,25 @@ __device__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, 
       const T nvis = bc + (T(4.9) / nc) * (nhe - nhw);
       fl = (fl + (ndz * nvis + (nvis > T(0.0) ? nhe : nhw) * nvis)) / T(2.0);
     }
-    if (xf)
+    // face cache for phase UV: each face is written by the one tile that owns it
+    const int n = g.n;
+    T* fc;
+    if (xf) {
       s_fu[fi] = fl;
-    else
+      fc = (a < b.ni || b.i0 + b.ni == m - kHalo)
+               ? io.fx + 3 * (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q))
+               : nullptr;
+    } else {
       s_fv[fi] = fl;
+      fc = (q < b.nj || b.j0 + b.nj == m - kHalo)
+               ? io.fy + 3 * (((long)f * n + (b.i0 - kHalo + a)) * (n + 1) + (b.j0 - kHalo + q))
+               : nullptr;
+    }
+    if (fc) {
+      fc[0] = bc;
+      fc[1] = vis;
+      fc[2] = T(0.5) * cc * (ue - uw);   // celerity viscosity flux, barotr_pure.py:68-69
+    }
   }
   __syncthreads();
 
@@ -675,46 +695,80 @@ __device__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, 
 }
 
 // Phase UV of one tile: writes the new u, v on the tile's interior cells.
-// io.h_out must hold the new h of every face (interior) from phase H.
+// io.h_out must hold the new h of every face (interior) and io.fx / io.fy the
+// face cache of this stage, both from phase H.
 template <typename T, int TI, int TJ>
 __device__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
-  const int m = g.m, f = b.f, tid = threadIdx.x;
-  T* s_h = sm;
-  T* s_u = s_h + S::R;
-  T* s_v = s_u + S::R;
-  T* s_g = s_v + S::R;      // [R][4]
-  T* s_s = s_g + 4 * S::R;
-  T* s_uc = s_s + S::R;
-  T* s_vc = s_uc + S::R;
-  T* s_hn = s_vc + S::R;    // new h, then the blended h of the pressure gradient
-  T* s_ku = s_hn + S::R;    // x faces [TI+1][TJ]: kinetic energy, tangential v, viscous flux
-  T* s_vx = s_ku + S::FX;
-  T* s_fx = s_vx + S::FX;
-  T* s_dzx = s_fx + S::FX;
-  T* s_cdy = s_dzx + S::FX;
-  T* s_kv = s_cdy + S::FX;  // y faces [TI][TJ+1]
-  T* s_uy = s_kv + S::FY;
-  T* s_fy = s_uy + S::FY;
-  T* s_dzy = s_fy + S::FY;
-  T* s_ddx = s_dzy + S::FY;
-  T* s_rda = s_ddx + S::FY; // cells [TI][TJ]
+  const int m = g.m, n = g.n, f = b.f, tid = threadIdx.x;
+  T* s_g = sm;              // cells [C][4] gct (16-byte aligned for cp.async)
+  T* s_s = s_g + 4 * S::C;  // cells: sina
+  T* s_rda = s_s + S::C;
   T* s_rdx = s_rda + S::C;
   T* s_rdy = s_rdx + S::C;
   T* s_af = s_rdy + S::C;
   T* s_up = s_af + S::C;
   T* s_vp = s_up + S::C;
-  T* s_np = s_vp + S::C;    // [NE][6] neighbour line: contravariant normal velocity
+  T* s_u = s_vp + S::C;     // region: raw u, v, new h (then the blended h), stage h
+  T* s_v = s_u + S::R;
+  T* s_hn = s_v + S::R;
+  T* s_h = s_hn + S::R;
+  T* s_xc = s_h + S::R;     // x faces [TI+1][TJ]: cache (3), kinetic energy, tangential v, c_dy
+  T* s_ku = s_xc + 3 * S::FX;
+  T* s_vx = s_ku + S::FX;
+  T* s_cdy = s_vx + S::FX;
+  T* s_yc = s_cdy + S::FX;  // y faces [TI][TJ+1]: cache (3), kinetic energy, tangential u, d_dx
+  T* s_kv = s_yc + 3 * S::FY;
+  T* s_uy = s_kv + S::FY;
+  T* s_ddx = s_uy + S::FY;
+  const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
 
-  stage_region_consts<T, TI, TJ>(g, b, s_g, s_s);
-  stage_consts<T, TI, TJ, true>(g, b, s_dzx, s_cdy, s_dzy, s_ddx, s_rda, s_rdx, s_rdy, s_af);
+  // constants (before the dependency on phase H)
+  for (int e = tid; e < S::C; e += kTileThreads) {
+    const int a = e / TJ, q = e % TJ;
+    if (a >= b.ni || q >= b.nj) continue;
+    const long o = cell(f, b.i0 + a, b.j0 + q, m);
+    cp_async_mat(s_g + 4 * e, g.gct + 4 * o);
+    cp_async_t(s_s + e, g.sina + o);
+    cp_async_t(s_rda + e, g.rda + o);
+    cp_async_t(s_rdx + e, g.rdx + o);
+    cp_async_t(s_rdy + e, g.rdy + o);
+    cp_async_t(s_af + e, g.a_f + o);
+  }
+  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
+    if (e < S::FX) {
+      const int a = e / TJ, q = e % TJ;
+      if (a <= b.ni && q < b.nj) cp_async_t(s_cdy + e, g.c_dy + cell(f, b.i0 + a, b.j0 + q, m));
+    } else {
+      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
+      if (a < b.ni && q <= b.nj) cp_async_t(s_ddx + e2, g.d_dx + cell(f, b.i0 + a, b.j0 + q, m));
+    }
+  }
   int cnt[4];
   const int P = edge_count(b, m, cnt);
   Gather<T, TI, TJ, true> gat;
   if (P > 0) gat.descriptors(g, io, b, cnt, P);
   wait_prior_grid();
-  stage_region_state<T, TI, TJ, true>(g, io, b, s_h, s_u, s_v, s_hn);
+
+  // state: region u, v, new h (and h), cells' base velocities, the face cache
+  const T* hn_src = (const T*)io.h_out;
+#pragma unroll
+  for (int it = 0; it < S::NIT; ++it) {
+    const int e = tid + it * kTileThreads;
+    if (e >= S::R) break;
+    const int r = e / RJ, c = e - r * RJ;
+    if (!region_needed(r, c, b.ni, b.nj)) continue;
+    const int i = b.i0 - kHalo + r, j = b.j0 - kHalo + c;
+    const long o = cell(f, i, j, m);
+    const bool inner = is_interior(i, j, m);
+    if (io.stored_halo || inner) {
+      cp_async_t(s_u + e, io.u + o);
+      cp_async_t(s_v + e, io.v + o);
+      if (blend) cp_async_t(s_h + e, io.h + o);
+    }
+    if (inner) cp_async_t(s_hn + e, hn_src + o);
+  }
   for (int e = tid; e < S::C; e += kTileThreads) {
     const int a = e / TJ, q = e % TJ;
     if (a >= b.ni || q >= b.nj) continue;
@@ -722,67 +776,56 @@ __device__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
     cp_async_t(s_up + e, io.up + o);
     cp_async_t(s_vp + e, io.vp + o);
   }
-  if (P > 0) gat.sources(g, io, b, cnt, P, s_h, s_u, s_v, s_hn, s_np, nullptr, nullptr);
+  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
+    const T* src;
+    T* dst;
+    if (e < S::FX) {
+      const int a = e / TJ, q = e % TJ;
+      if (a > b.ni || q >= b.nj) continue;
+      src = io.fx + 3 * (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q));
+      dst = s_xc + 3 * e;
+    } else {
+      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
+      if (a >= b.ni || q > b.nj) continue;
+      src = io.fy + 3 * (((long)f * n + (b.i0 - kHalo + a)) * (n + 1) + (b.j0 - kHalo + q));
+      dst = s_yc + 3 * e2;
+    }
+    cp_async_t(dst, src);
+    cp_async_t(dst + 1, src + 1);
+    cp_async_t(dst + 2, src + 2);
+  }
+  if (P > 0) gat.sources(g, io, b, cnt, P, s_h, s_u, s_v, s_hn, nullptr, nullptr, nullptr);
   cp_async_wait_all();
   __syncthreads();
 
+  if (blend) {
 #pragma unroll
-  for (int it = 0; it < S::NIT; ++it) {
-    const int e = tid + it * kTileThreads;
-    if (e >= S::R) break;
-    const int r = e / RJ, c = e - r * RJ;
-    if (!region_needed(r, c, b.ni, b.nj)) continue;
-    const T* G = s_g + 4 * e;
-    const T u = s_u[e], v = s_v[e], sn = s_s[e];
-    s_uc[e] = (G[0] * u + G[1] * v) * sn;
-    s_vc[e] = (G[2] * u + G[3] * v) * sn;
-    s_hn[e] = (T(1.0) - io.beta) * s_hn[e] + io.beta * s_h[e];  // fb_scheme, barotr_pure.py:52-54
-  }
-  __syncthreads();
-
-  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
-    const bool xf = e < S::FX;
-    int a, q, stride, base, side, kind, pos, fi;
-    if (xf) {
-      a = e / TJ;
-      q = e % TJ;
-      if (a > b.ni || q >= b.nj) continue;
-      stride = RJ;
-      base = a * RJ + (q + kHalo);
-      side = xface_side(b.i0 + a, m);
-      kind = side == kS ? 0 : 1;
-      pos = q;
-      fi = e;
-    } else {
-      fi = e - S::FX;
-      a = fi / (TJ + 1);
-      q = fi % (TJ + 1);
-      if (a >= b.ni || q > b.nj) continue;
-      stride = 1;
-      base = (a + kHalo) * RJ + q;
-      side = yface_side(b.j0 + q, m);
-      kind = side == kW ? 2 : 3;
-      pos = a;
+    for (int it = 0; it < S::NIT; ++it) {
+      const int e = tid + it * kTileThreads;
+      if (e >= S::R) break;
+      const int r = e / RJ, c = e - r * RJ;
+      if (!region_needed(r, c, b.ni, b.nj)) continue;
+      s_hn[e] = (T(1.0) - io.beta) * s_hn[e] + io.beta * s_h[e];  // fb_scheme, barotr_pure.py:52-54
     }
-    const T* ph = s_h + base;
-    const T* pn = (xf ? s_uc : s_vc) + base;   // normal contravariant component
-    const T* pt = (xf ? s_v : s_u) + base;     // raw tangential component (remap.py:84-94)
-    const T ue = rplus(pn, stride), uw = rminus(pn + stride, stride);
-    T bc = T(0.5) * (ue + uw);
-    if (side >= 0) bc = (bc + line_raw(s_np + 6 * (kind * S::EW + pos))) / T(2.0);
-    const T vt = bc > T(0.0) ? rplus(pt, stride) : rminus(pt + stride, stride);
-    const T cc = celerity(mid6(ph, stride), xf ? s_dzx[fi] : s_dzy[fi]);
-    const T vis = bc + (T(4.9) / cc) * (rplus(ph, stride) - rminus(ph + stride, stride));
-    const T kin = T(0.5) * (vis * vis + vt * vt);
-    const T fvis = T(0.5) * cc * (ue - uw);   // barotr_pure.py:68-69
-    if (xf) {
-      s_ku[fi] = kin;
-      s_vx[fi] = vt;
-      s_fx[fi] = fvis;
+  }
+  // faces: upwind tangential component (remap.py:73-95) and kinetic energy (barotr_pure.py:91-92)
+  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
+    if (e < S::FX) {
+      const int a = e / TJ, q = e % TJ;
+      if (a > b.ni || q >= b.nj) continue;
+      const T* pt = s_v + a * RJ + (q + kHalo);
+      const T* c = s_xc + 3 * e;
+      const T vt = c[0] > T(0.0) ? rplus(pt, RJ) : rminus(pt + RJ, RJ);
+      s_ku[e] = T(0.5) * (c[1] * c[1] + vt * vt);
+      s_vx[e] = vt;
     } else {
-      s_kv[fi] = kin;
-      s_uy[fi] = vt;
-      s_fy[fi] = fvis;
+      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
+      if (a >= b.ni || q > b.nj) continue;
+      const T* pt = s_u + (a + kHalo) * RJ + q;
+      const T* c = s_yc + 3 * e2;
+      const T ut = c[0] > T(0.0) ? rplus(pt, 1) : rminus(pt + 1, 1);
+      s_kv[e2] = T(0.5) * (c[1] * c[1] + ut * ut);
+      s_uy[e2] = ut;
     }
   }
   __syncthreads();
@@ -794,25 +837,27 @@ __device__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
     const int xf0 = e, xf1 = e + TJ;
     const int yf0 = a * (TJ + 1) + q, yf1 = yf0 + 1;
     const int lc = (a + kHalo) * RJ + (q + kHalo);
-    const T uct = s_uc[lc], vct = s_vc[lc];
-    const T rdx = s_rdx[xf0], rdy = s_rdy[xf0];
+    const T* G = s_g + 4 * e;
+    const T u = s_u[lc], v = s_v[lc], sn = s_s[e];
+    const T uct = (G[0] * u + G[1] * v) * sn, vct = (G[2] * u + G[3] * v) * sn;  // remap.py:34-39
+    const T rdx = s_rdx[e], rdy = s_rdy[e];
     // vorticity (agrid.py:31-41) and advection (barotr_pure.py:78-97)
-    const T vort = s_rda[xf0] * (s_uy[yf0] * s_ddx[yf0] + s_vx[xf1] * s_cdy[xf1] - s_uy[yf1] * s_ddx[yf1] -
-                                 s_vx[xf0] * s_cdy[xf0]);
+    const T vort = s_rda[e] * (s_uy[yf0] * s_ddx[yf0] + s_vx[xf1] * s_cdy[xf1] - s_uy[yf1] * s_ddx[yf1] -
+                               s_vx[xf0] * s_cdy[xf0]);
     const T advx = vort * vct - (s_ku[xf1] - s_ku[xf0]) * rdx;
     const T advy = -vort * uct - (s_kv[yf1] - s_kv[yf0]) * rdy;
-    // celerity viscosity (barotr_pure.py:63-75)
-    const T visx = -(rdx * (s_fx[xf1] - s_fx[xf0]));
-    const T visy = -(rdy * (s_fy[yf1] - s_fy[yf0]));
+    // celerity viscosity (barotr_pure.py:63-75) from the cached face fluxes
+    const T visx = -(rdx * (s_xc[3 * xf1 + 2] - s_xc[3 * xf0 + 2]));
+    const T visy = -(rdy * (s_yc[3 * yf1 + 2] - s_yc[3 * yf0 + 2]));
     // pressure gradient of the new h (agrid.py:55-69, barotr_pure.py:57-60)
     const T* pbx = s_hn + (a * RJ + (q + kHalo));
     const T* pby = s_hn + ((a + kHalo) * RJ + q);
     const T pgu = T(-9.80) * (rdx * (mid6(pbx + RJ, RJ) - mid6(pbx, RJ)));
     const T pgv = T(-9.80) * (rdy * (mid6(pby + 1, 1) - mid6(pby, 1)));
-    const T af = s_af[xf0];
+    const T af = s_af[e];
     // momentum update (barotr_pure.py:149-150)
-    io.u_out[o] = s_up[xf0] + (pgu + advx + af * vct + visx) * io.dt;
-    io.v_out[o] = s_vp[xf0] + (pgv + advy - af * uct + visy) * io.dt;
+    io.u_out[o] = s_up[e] + (pgu + advx + af * vct + visx) * io.dt;
+    io.v_out[o] = s_vp[e] + (pgv + advy - af * uct + visy) * io.dt;
   }
 }
 
@@ -871,6 +916,8 @@ __device__ StageIO<T> round_stage(const RoundArgs<T>& a, int step, int st) {
   io.h_out = out[0];
   io.u_out = out[1];
   io.v_out = out[2];
+  io.fx = a.fx;
+  io.fy = a.fy;
   double dt;
   if (a.rk == 2) {
     dt = st == 0 ? a.dtb / 2.0 : a.dtb;      // barotr.py:50-56
