@@ -39,6 +39,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 B_ALG_WORDS = 41  # algorithmic words per cell-update (both RK stages), see DESIGN.md
+# Compulsory words per interior cell of each phase kernel, averaged over the two
+# RK2 stages (stage 1 / stage 2): distinct field reads + writes of the kernel's work.
+#   phase H : h, u, v, [h base], dzph_x, dzph_y, gct(4), sina, rda, c_dy, d_dx -> h     14 / 15
+#   phase UV: u, v, h, new h, [u, v base], gct(4), sina, rda, rdx, rdy, a_f, c_dy,
+#             d_dx, dzph_x, dzph_y -> u, v                                          18 / 20
+KERNEL_WORDS = {"phase_h": 14.5, "phase_uv": 19.0}
+KERNEL_NAMES = {"phase_h": "k_phase_h", "phase_uv": "k_phase_uv"}
 METRIC = "barotropic cell-updates/s"
 UNIT = "cell-updates/s"
 
@@ -58,7 +65,29 @@ def parse_args():
     p.add_argument("--cpu-substeps", type=int, default=60,
                    help="substeps of the bounded CPU baseline sample")
     p.add_argument("--no-extras", action="store_true", help="skip the fp32 / mode comparison lines")
+    p.add_argument("--case-only", action="store_true",
+                   help="run one round of --nbb substeps (the profiling target) and exit, no timing")
+    p.add_argument("--dtype", default="f64", choices=["f64", "f32"], help="dtype of --case-only")
     return p.parse_args()
+
+
+def run_case(args):
+    """One round of the workload in the given mode/tile: the target of ncu captures."""
+    import torch
+    from licom4py_gpu_b200.plan import BtPlan
+    _, consts, st, dtb = build_problem(args.n, args.depth, args.seed)
+    dtype = torch.float64 if args.dtype == "f64" else torch.float32
+    tile = (8, 16) if args.tile == "auto" else tuple(int(x) for x in args.tile.split("x"))
+    mode = "stream" if args.mode == "auto" else args.mode
+    p = BtPlan(consts, dtype=dtype, tile=tile, mode=mode)
+    h = torch.from_numpy(st["h0"]).cuda().to(dtype)
+    u = torch.from_numpy(st["ub"]).cuda().to(dtype)
+    v = torch.from_numpy(st["vb"]).cuda().to(dtype)
+    out = p.round(h, h, u, v, u, v, nbb=args.nbb, dtb=dtb)
+    torch.cuda.synchronize()
+    p.check_device_error()
+    print(json.dumps({"case": f"C{args.n}", "dtype": args.dtype, "mode": mode, "tile": list(tile),
+                      "nbb": args.nbb, "h_absmax": float(out["h0"].abs().max())}))
 
 
 def dist_setup(args):
@@ -266,7 +295,7 @@ def run_ours(args, world, rank, local):
     value = world * cells * nbb * args.steps / (ms * 1e-3)
     launches_per_step = {"persistent": 4, "graph": 4 * nbb + 3, "stream": 4 * nbb + 3}[mode]
 
-    # roofline of the dominant kernel (the persistent round kernel: one launch per step)
+    # roofline of the dominant kernel
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -275,21 +304,46 @@ def run_ours(args, world, rank, local):
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    roofline = None
-    if mode == "persistent" and klaunch:
-        alg_bytes = B_ALG_WORDS * 8 * cells * nbb
-        achieved = alg_bytes / (kms / klaunch * 1e-3) / 1e9
+
+    def kernel_roofline(nn, dtype, tile_, nbb_, consts_, st_, dtb_):
+        """Events around every phase kernel (stream mode, same stream) over one round."""
+        p = BtPlan(consts_, dtype=dtype, device=dev, tile=tile_, mode="stream")
+        h = torch.from_numpy(st_["h0"]).to(dev, dtype)
+        u = torch.from_numpy(st_["ub"]).to(dev, dtype)
+        v = torch.from_numpy(st_["vb"]).to(dev, dtype)
+        o = {k: p.empty_field() for k in ("h0", "ub", "vb") + DIAG_NAMES}
+        p.round(h, h, u, v, u, v, nbb=min(nbb_, 50), dtb=dtb_, out=o)
+        p.enable_kernel_timing(True)
+        flush.fill_(0.0)
+        p.round(h, h, u, v, u, v, nbb=nbb_, dtb=dtb_, out=o)
+        torch.cuda.synchronize()
+        res = {k: p.kernel_time(k) for k in ("phase_h", "phase_uv")}
+        p.close()
+        tot = sum(ms for ms, _ in res.values())
+        dom = max(res, key=lambda k: res[k][0])
+        ms, nl = res[dom]
+        esz = 8 if dtype == torch.float64 else 4
+        alg = KERNEL_WORDS[dom] * esz * 6 * nn * nn
+        achieved = alg / (ms / nl * 1e-3) / 1e9
         traffic = None
-        tfile = os.path.join(ROOT, "profiles", f"k_round_c{n}_f64_traffic.json")
+        tfile = os.path.join(ROOT, "profiles", f"{KERNEL_NAMES[dom]}_c{nn}_{'f64' if esz == 8 else 'f32'}.json")
         if os.path.exists(tfile):
             try:
-                tj = json.load(open(tfile))
-                traffic = tj.get("dram_bytes_per_launch_scaled", {}).get(str(nbb))
+                traffic = json.load(open(tfile)).get("dram_bytes_per_launch")
             except (OSError, ValueError):
                 traffic = None
-        roofline = {"bound": "hbm", "kernel": "k_round<double>", "achieved": achieved, "peak": peak,
-                    "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                    "kernel_ms": kms / klaunch, "alg_bytes_per_launch": alg_bytes}
+        return {"bound": "hbm", "kernel": f"{KERNEL_NAMES[dom]}<{'double' if esz == 8 else 'float'},"
+                                          f"{tile_[0]},{tile_[1]}>",
+                "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "launch_us": 1e3 * ms / nl,
+                "alg_bytes_per_launch": alg, "launches_timed": nl,
+                "share_of_phase_time": {k: res[k][0] / tot for k in res}}
+
+    roofline = kernel_roofline(n, torch.float64, tile, nbb, consts, st, dtb)
+    round_roofline = {"achieved": B_ALG_WORDS * 8 * cells * nbb / (ms_per_step * 1e-3) / 1e9,
+                      "peak": peak, "unit": "GB/s",
+                      "frac": B_ALG_WORDS * 8 * cells * nbb / (ms_per_step * 1e-3) / 1e9 / peak,
+                      "bytes_per_cell_update": B_ALG_WORDS * 8}
 
     # end to end through the public call, host (pinned) buffers
     pinned_in = [torch.from_numpy(a).pin_memory() for a in (st["h0"], st["h0"], st["ub"], st["vb"], st["ub"], st["vb"])]
@@ -349,6 +403,26 @@ def run_ours(args, world, rank, local):
             modes[md] = {"value": cells * nbb * steps / (msm * 1e-3), "ms_per_step": msm / steps}
             pm.close()
         extras["modes_f64"] = modes
+        # the HBM-bound size: C384 rounds (float64 and float32), graph mode, tuned tile
+        g384, c384, s384, d384 = build_problem(384, args.depth, args.seed)
+        big = {}
+        for dt_, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
+            cfg384 = choose_config(384, dt_, consts=c384, device=dev)
+            t384 = tuple(cfg384["tile"])
+            p = BtPlan(c384, dtype=dt_, device=dev, tile=t384, mode="graph")
+            hh = torch.from_numpy(s384["h0"]).to(dev, dt_)
+            uu = torch.from_numpy(s384["ub"]).to(dev, dt_)
+            vv = torch.from_numpy(s384["vb"]).to(dev, dt_)
+            ins384 = [hh, hh, uu, vv, uu, vv]
+            o384 = {k: p.empty_field() for k in ("h0", "ub", "vb") + DIAG_NAMES}
+            msb, _ = timed_rounds(p, ins384, o384, 3, 2)
+            p.close()
+            cu = 6 * 384 * 384 * nbb * 3 / (msb * 1e-3)
+            esz = 8 if tag == "f64" else 4
+            big[tag] = {"value": cu, "unit": UNIT, "ms_per_step": msb / 3, "tile": list(t384),
+                        "round_frac_of_hbm": cu * B_ALG_WORDS * esz / 1e9 / peak,
+                        "kernel": kernel_roofline(384, dt_, t384, 100, c384, s384, d384)}
+        extras["c384"] = big
 
     cpu = None
     if rank == 0 and world == 1:
@@ -364,7 +438,7 @@ def run_ours(args, world, rank, local):
                            "parallelism": f"replicas x{world}",
                            "l2": "flushed between steps (512 MiB write outside the timed windows); "
                                  "within a step the member's working set stays L2-resident"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "round_roofline": round_roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
         line.update(extras)
         print(json.dumps(line), flush=True)
@@ -373,6 +447,9 @@ def run_ours(args, world, rank, local):
 
 def main():
     args = parse_args()
+    if args.case_only:
+        run_case(args)
+        return
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -47,7 +47,13 @@ extern "C" {
 /* Plan options (bt_plan_set_option) */
 #define BT_OPT_MAX_CTAS 1    /* persistent mode: cap on the cooperative grid (0 = occupancy limit) */
 #define BT_OPT_SPIN_LIMIT 2  /* persistent mode: polls a grid-barrier wait may take before it gives up */
-#define BT_OPT_KERNEL_TIMING 3  /* persistent mode: 1 = bracket each round kernel with CUDA events */
+#define BT_OPT_KERNEL_TIMING 3  /* 1 = bracket the round kernel (persistent mode) or each phase kernel
+                                   (stream mode) with CUDA events on its stream; setting it resets the record */
+
+/* Kernel kinds of bt_plan_kernel_time */
+#define BT_KERNEL_ROUND 0     /* the persistent round kernel */
+#define BT_KERNEL_PHASE_H 1   /* the h-update tile kernel of a stage */
+#define BT_KERNEL_PHASE_UV 2  /* the momentum-update tile kernel of a stage */
 
 /* Plan information (bt_plan_get_info) */
 #define BT_INFO_LAST_GRID 1      /* CTAs of the last persistent launch */
@@ -121,9 +127,9 @@ int bt_plan_set_mode(bt_plan* plan, int mode);
  * waiting forever; bt_check_device_error then reports BT_EDEVICE. */
 int bt_plan_set_option(bt_plan* plan, int key, long long value);
 
-/* Sum of the durations of the round kernels launched since timing was
- * enabled or last read (BT_OPT_KERNEL_TIMING); waits for them; resets the sum. */
-int bt_plan_kernel_time(bt_plan* plan, double* ms_total, int* launches);
+/* Sum of the durations of the timed kernels of one kind (BT_KERNEL_*) launched
+ * since BT_OPT_KERNEL_TIMING was last set; waits for them. */
+int bt_plan_kernel_time(bt_plan* plan, int kind, double* ms_total, int* launches);
 
 /* Read plan information (BT_INFO_*); -1 for an unknown key. */
 long long bt_plan_get_info(bt_plan* plan, int key);
@@ -162,6 +168,19 @@ int bt_edge_average(bt_plan* plan, void* u, void* v, void* stream);
  * (cube.py:40-153) and the halo routing of communication.py:269-474. */
 int bt_halo_table_host(int n, const double* k2e_coef, const int* loc_i, const int* loc_j, int* src,
                        double* weights, int* route);
+
+/* Interior statistics of a (6, n+6, n+6) field: out3 (device, 3 float64) =
+ * max, min, mean over the 6 n^2 interior cells; the global diagnostic of
+ * src/licom/mymodule/diag.py:45-75 computed on the device.  Deterministic. */
+int bt_interior_stats(int n, int dtype, const void* field, void* out3, void* stream);
+
+/* Conservation sums over the interior: out2 (device, 2 float64) = total mass
+ * sum(h da) and energy sum((g h^2 / 2 + (depth + h) |u_lonlat|^2 / 2) da),
+ * da = 1 / rda, u_lonlat = a_c2l . (u, v).  Terms in the fields' precision,
+ * sums compensated in float64, fixed reduction order (deterministic).
+ * No counterpart in the reference (its diagnostics stop at max/min/mean). */
+int bt_conservation(int n, int dtype, const void* h, const void* u, const void* v, const void* rda,
+                    const void* a_c2l, double depth, void* out2, void* stream);
 
 /* Synchronise the plan's work and report a device-side error flag, if set. */
 int bt_check_device_error(bt_plan* plan);

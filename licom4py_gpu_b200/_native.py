@@ -17,6 +17,7 @@ BT_F64, BT_F32 = 0, 1
 BT_MODE_STREAM, BT_MODE_GRAPH, BT_MODE_PERSISTENT = 0, 1, 2
 BT_OPT_MAX_CTAS, BT_OPT_SPIN_LIMIT, BT_OPT_KERNEL_TIMING = 1, 2, 3
 BT_INFO_LAST_GRID, BT_INFO_SCRATCH_BYTES = 1, 2
+BT_KERNEL_ROUND, BT_KERNEL_PHASE_H, BT_KERNEL_PHASE_UV = 0, 1, 2
 
 _vp = ctypes.c_void_p
 
@@ -45,7 +46,8 @@ _lib = None
 # every symbol declared in include/licom_bt.h
 EXPORTS = ("bt_plan_create", "bt_plan_destroy", "bt_plan_set_tile", "bt_plan_set_mode",
            "bt_plan_set_option", "bt_plan_get_info", "bt_plan_kernel_time", "bt_round",
-           "bt_stage", "bt_fill_halo", "bt_edge_average", "bt_check_device_error", "bt_halo_table_host", "bt_last_error", "bt_version")
+           "bt_stage", "bt_fill_halo", "bt_edge_average", "bt_check_device_error", "bt_halo_table_host", "bt_interior_stats", "bt_conservation",
+           "bt_last_error", "bt_version")
 
 
 def lib():
@@ -64,7 +66,8 @@ def lib():
     L.bt_plan_set_mode.argtypes = [_vp, ctypes.c_int]
     L.bt_plan_set_option.argtypes = [_vp, ctypes.c_int, ctypes.c_longlong]
     L.bt_plan_get_info.argtypes = [_vp, ctypes.c_int]
-    L.bt_plan_kernel_time.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    L.bt_plan_kernel_time.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_int)]
     L.bt_round.argtypes = [_vp, ctypes.POINTER(StateIn), ctypes.POINTER(StateOut), ctypes.c_int,
                            ctypes.c_double, ctypes.c_int, _vp]
     L.bt_stage.argtypes = [_vp, ctypes.POINTER(StateIn), ctypes.POINTER(StateOut), ctypes.c_double,
@@ -73,6 +76,8 @@ def lib():
     L.bt_edge_average.argtypes = [_vp, _vp, _vp, _vp]
     L.bt_check_device_error.argtypes = [_vp]
     L.bt_halo_table_host.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.bt_interior_stats.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
+    L.bt_conservation.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _vp]
     L.bt_last_error.argtypes = []
     L.bt_last_error.restype = ctypes.c_char_p
     L.bt_version.argtypes = []

@@ -14,13 +14,19 @@
 using namespace bt;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
 
-int fail(int code, const std::string& msg) {
+namespace bt {
+int set_error(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
+}  // namespace bt
+
+namespace {
+
+int fail(int code, const std::string& msg) { return set_error(code, msg); }
 
 int cuda_fail(cudaError_t e, const char* what) {
   return fail(BT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -100,10 +106,32 @@ struct bt_plan {
   int max_ctas = 0;
   long long spin_limit = 1ll << 24;
   int last_grid = 0;
-  // optional timing of the main round kernel (persistent mode): event pairs on the launch stream
+  // optional kernel timing: event pairs on the launch stream around the round
+  // kernel (persistent mode) or each phase kernel (stream mode), with their kind
   int timing = 0;
-  std::vector<cudaEvent_t> tev;
-  size_t tev_used = 0;
+  mutable std::vector<cudaEvent_t> tev;
+  mutable std::vector<int> tkind;
+  mutable size_t tev_used = 0;
+
+  // Record the start event of a timed kernel of the given kind (nullptr if timing is off).
+  cudaError_t time_begin(int kind, cudaStream_t s, cudaEvent_t* stop) const {
+    *stop = nullptr;
+    if (!timing) return cudaSuccess;
+    if (tev_used + 2 > tev.size()) {
+      for (int k = 0; k < 2; ++k) {
+        cudaEvent_t ev;
+        cudaError_t e = cudaEventCreate(&ev);
+        if (e != cudaSuccess) return e;
+        tev.push_back(ev);
+      }
+    }
+    tkind.resize(tev.size() / 2);
+    tkind[tev_used / 2] = kind;
+    cudaEvent_t start = tev[tev_used];
+    *stop = tev[tev_used + 1];
+    tev_used += 2;
+    return cudaEventRecord(start, s);
+  }
 
   size_t esize() const { return dtype == BT_F64 ? 8 : 4; }
   // scratch layout: 6 stage fields, edge lines (24 n), face caches x and y (6 (n+1) n 3 each)
@@ -258,9 +286,14 @@ StageIO<T> stage_io(const bt_plan* p, const T* h, const T* u, const T* v, const 
 
 template <typename T>
 cudaError_t run_stage(const bt_plan* p, const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
-  cudaError_t e = launch_phase_h<T>(g, io, p->tile, s);
-  if (e != cudaSuccess) return e;
-  return launch_phase_uv<T>(g, io, p->tile, s);
+  cudaEvent_t stop;
+  cudaError_t e = p->time_begin(BT_KERNEL_PHASE_H, s, &stop);
+  if (e == cudaSuccess) e = launch_phase_h<T>(g, io, p->tile, s);
+  if (e == cudaSuccess && stop) e = cudaEventRecord(stop, s);
+  if (e == cudaSuccess) e = p->time_begin(BT_KERNEL_PHASE_UV, s, &stop);
+  if (e == cudaSuccess) e = launch_phase_uv<T>(g, io, p->tile, s);
+  if (e == cudaSuccess && stop) e = cudaEventRecord(stop, s);
+  return e;
 }
 
 // The launch sequence of one round (stream order).
@@ -359,20 +392,8 @@ cudaError_t enqueue_round_persistent(bt_plan* p, const bt_state_in& in, const bt
   a.spin_limit = p->spin_limit;
   cudaError_t e = cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  cudaEvent_t t0 = nullptr, t1 = nullptr;
-  if (p->timing) {
-    if (p->tev_used + 2 > p->tev.size()) {
-      for (int k = 0; k < 2; ++k) {
-        cudaEvent_t ev;
-        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
-        p->tev.push_back(ev);
-      }
-    }
-    t0 = p->tev[p->tev_used];
-    t1 = p->tev[p->tev_used + 1];
-    p->tev_used += 2;
-    if ((e = cudaEventRecord(t0, s)) != cudaSuccess) return e;
-  }
+  cudaEvent_t t1 = nullptr;
+  if ((e = p->time_begin(BT_KERNEL_ROUND, s, &t1)) != cudaSuccess) return e;
   e = launch_round<T>(a, p->tile, p->max_ctas, s, &p->last_grid);
   if (e != cudaSuccess) return e;
   if (t1 && (e = cudaEventRecord(t1, s)) != cudaSuccess) return e;
@@ -674,18 +695,20 @@ int bt_plan_set_option(bt_plan* p, int key, long long value) {
   }
 }
 
-int bt_plan_kernel_time(bt_plan* p, double* ms_total, int* launches) {
+int bt_plan_kernel_time(bt_plan* p, int kind, double* ms_total, int* launches) {
   if (!p || !ms_total || !launches) return fail(BT_EINVAL, "bt_plan_kernel_time: NULL argument");
   double total = 0.0;
+  int count = 0;
   for (size_t k = 0; k + 1 < p->tev_used; k += 2) {
+    if (p->tkind[k / 2] != kind) continue;
     BT_CUDA(cudaEventSynchronize(p->tev[k + 1]), "bt_plan_kernel_time: synchronize");
     float ms = 0.f;
     BT_CUDA(cudaEventElapsedTime(&ms, p->tev[k], p->tev[k + 1]), "bt_plan_kernel_time: elapsed");
     total += ms;
+    ++count;
   }
   *ms_total = total;
-  *launches = (int)(p->tev_used / 2);
-  p->tev_used = 0;
+  *launches = count;
   return BT_OK;
 }
 

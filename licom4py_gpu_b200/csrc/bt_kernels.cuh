@@ -39,27 +39,51 @@ __global__ void __launch_bounds__(kThreads) k_phase_uv(Geo<T> g, StageIO<T> io, 
 }
 
 // One whole round of one member in a single cooperative launch: every CTA
-// walks the tiles of a phase, then all CTAs meet at a grid barrier.
+// walks its tiles of a phase, then all CTAs meet at a grid barrier.  Before
+// waiting at the barrier a CTA already issues the next phase's prologue for
+// its first tile (constants by cp.async, halo descriptors), so those loads
+// overlap the barrier.
 template <typename T, int TI, int TJ>
-__global__ void __launch_bounds__(kThreads, 2) k_round(RoundArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, 3) k_round(RoundArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const int ntiles = 6 * a.t.tiles_per_face();
   const int nst = a.rk == 2 ? 2 : 3;
+  const int nphase = a.nbb * nst * 2;
+  const int t0 = blockIdx.x;
   unsigned gen = 0;
-  for (int step = 0; step < a.nbb; ++step) {
-    for (int st = 0; st < nst; ++st) {
-      const StageIO<T> io = round_stage(a, step, st);
-      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        tile_h<T, TI, TJ>(a.g, io, tile_box(a.t, a.g.n, tile), sm);
-        __syncthreads();
+  Gather<T, TI, TJ, false> gh;
+  Gather<T, TI, TJ, true> gu;
+  int cnt[4], P = 0;
+  if (t0 < ntiles) tile_h_pro<T, TI, TJ>(a.g, round_stage(a, 0, 0), tile_box(a.t, a.g.n, t0), sm, gh, cnt, P);
+  for (int ph = 0; ph < nphase; ++ph) {
+    const int step = ph / (2 * nst), st = (ph >> 1) % nst;
+    const bool uv = ph & 1;
+    const StageIO<T> io = round_stage(a, step, st);
+    int k = 0;
+    for (int tile = t0; tile < ntiles; tile += gridDim.x, ++k) {
+      const TileBox b = tile_box(a.t, a.g.n, tile);
+      if (!uv) {
+        if (k > 0) tile_h_pro<T, TI, TJ>(a.g, io, b, sm, gh, cnt, P);
+        tile_h_main<T, TI, TJ>(a.g, io, b, sm, gh, cnt, P);
+      } else {
+        if (k > 0) tile_uv_pro<T, TI, TJ>(a.g, io, b, sm, gu, cnt, P);
+        tile_uv_main<T, TI, TJ>(a.g, io, b, sm, gu, cnt, P);
       }
-      if (!grid_barrier(a.bar, gen, a.err, a.spin_limit)) return;
-      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        tile_uv<T, TI, TJ>(a.g, io, tile_box(a.t, a.g.n, tile), sm);
-        __syncthreads();
-      }
-      if (!grid_barrier(a.bar, gen, a.err, a.spin_limit)) return;
+      __syncthreads();
+    }
+    if (ph + 1 < nphase && t0 < ntiles) {
+      const int nx = ph + 1, nstep = nx / (2 * nst), nst2 = (nx >> 1) % nst;
+      const StageIO<T> io_n = round_stage(a, nstep, nst2);
+      const TileBox b = tile_box(a.t, a.g.n, t0);
+      if (nx & 1)
+        tile_uv_pro<T, TI, TJ>(a.g, io_n, b, sm, gu, cnt, P);
+      else
+        tile_h_pro<T, TI, TJ>(a.g, io_n, b, sm, gh, cnt, P);
+    }
+    if (!grid_barrier(a.bar, gen, a.err, a.spin_limit)) {
+      cp_async_wait_all();  // no copy may be left in flight when the CTA leaves
+      return;
     }
   }
 }

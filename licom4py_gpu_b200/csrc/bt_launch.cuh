@@ -1,10 +1,15 @@
 // bt_launch.cuh - host-side launch interface of the barotropic kernels (internal C++).
 #pragma once
 
+#include <string>
+
 #include "bt_common.cuh"
 #include "bt_stencil.cuh"
 
 namespace bt {
+
+// Record the thread-local message returned by bt_last_error(); returns code.
+int set_error(int code, const std::string& msg);
 
 struct TileCfg {
   int ti, tj;

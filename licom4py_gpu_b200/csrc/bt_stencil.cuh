@@ -559,39 +559,59 @@ __device__ __forceinline__ void stage_region_state(const Geo<T>& g, const StageI
   }
 }
 
+// Shared-memory layout of phase H (offsets in words).
+template <typename T, int TI, int TJ>
+struct LayoutH {
+  using S = TileShape<TI, TJ>;
+  T *s_h, *s_u, *s_v, *s_g, *s_s, *s_uc, *s_vc, *s_fu, *s_fv, *s_dzx, *s_cdy, *s_dzy, *s_ddx, *s_rda, *s_hp,
+      *s_np, *s_nh, *s_ndz;
+  __device__ __forceinline__ explicit LayoutH(T* sm) {
+    s_h = sm;
+    s_u = s_h + S::R;
+    s_v = s_u + S::R;
+    s_g = s_v + S::R;      // [R][4]
+    s_s = s_g + 4 * S::R;
+    s_uc = s_s + S::R;
+    s_vc = s_uc + S::R;
+    s_fu = s_vc + S::R;    // [TI+1][TJ] mass flux on x faces
+    s_fv = s_fu + S::FX;   // [TI][TJ+1] on y faces
+    s_dzx = s_fv + S::FY;  // [TI+1][TJ]
+    s_cdy = s_dzx + S::FX;
+    s_dzy = s_cdy + S::FX; // [TI][TJ+1]
+    s_ddx = s_dzy + S::FY;
+    s_rda = s_ddx + S::FY; // [TI][TJ]
+    s_hp = s_rda + S::C;
+    s_np = s_hp + S::C;    // [NE][6] neighbour line: contravariant normal velocity
+    s_nh = s_np + 6 * S::NE;   // [NE][6] neighbour line: h
+    s_ndz = s_nh + 6 * S::NE;  // [NE] neighbour depth at the edge face
+  }
+};
+
+// Phase H prologue: constants of the tile (cp.async, not yet awaited) and the
+// halo-gather descriptors.  Independent of the state, so it may run before the
+// previous phase has finished (programmatic launch, or before a grid barrier).
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                           Gather<T, TI, TJ, false>& gat, int* cnt, int& P) {
+  const LayoutH<T, TI, TJ> L(sm);
+  stage_region_consts<T, TI, TJ>(g, b, L.s_g, L.s_s);
+  stage_consts<T, TI, TJ, false>(g, b, L.s_dzx, L.s_cdy, L.s_dzy, L.s_ddx, L.s_rda, nullptr, nullptr, nullptr);
+  P = edge_count(b, g.m, cnt);
+  if (P > 0) gat.descriptors(g, io, b, cnt, P);
+}
+
 // Phase H of one tile: writes the new h on the tile's interior cells.
 template <typename T, int TI, int TJ>
-__device__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
+__device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                            Gather<T, TI, TJ, false>& gat, const int* cnt, int P) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
   const int m = g.m, f = b.f, tid = threadIdx.x;
-  T* s_h = sm;
-  T* s_u = s_h + S::R;
-  T* s_v = s_u + S::R;
-  T* s_g = s_v + S::R;      // [R][4]
-  T* s_s = s_g + 4 * S::R;
-  T* s_uc = s_s + S::R;
-  T* s_vc = s_uc + S::R;
-  T* s_fu = s_vc + S::R;    // [TI+1][TJ] mass flux on x faces
-  T* s_fv = s_fu + S::FX;   // [TI][TJ+1] on y faces
-  T* s_dzx = s_fv + S::FY;  // [TI+1][TJ]
-  T* s_cdy = s_dzx + S::FX;
-  T* s_dzy = s_cdy + S::FX; // [TI][TJ+1]
-  T* s_ddx = s_dzy + S::FY;
-  T* s_rda = s_ddx + S::FY; // [TI][TJ]
-  T* s_hp = s_rda + S::C;
-  T* s_np = s_hp + S::C;    // [NE][6] neighbour line: contravariant normal velocity
-  T* s_nh = s_np + 6 * S::NE;   // [NE][6] neighbour line: h
-  T* s_ndz = s_nh + 6 * S::NE;  // [NE] neighbour depth at the edge face
-
-  // constants first: they do not depend on the previous kernel
-  stage_region_consts<T, TI, TJ>(g, b, s_g, s_s);
-  stage_consts<T, TI, TJ, false>(g, b, s_dzx, s_cdy, s_dzy, s_ddx, s_rda, nullptr, nullptr, nullptr);
-  int cnt[4];
-  const int P = edge_count(b, m, cnt);
-  Gather<T, TI, TJ, false> gat;
-  if (P > 0) gat.descriptors(g, io, b, cnt, P);
-  wait_prior_grid();
+  const LayoutH<T, TI, TJ> L(sm);
+  T* s_h = L.s_h;
+  T *s_u = L.s_u, *s_v = L.s_v, *s_g = L.s_g, *s_s = L.s_s, *s_uc = L.s_uc, *s_vc = L.s_vc;
+  T *s_fu = L.s_fu, *s_fv = L.s_fv, *s_dzx = L.s_dzx, *s_cdy = L.s_cdy, *s_dzy = L.s_dzy, *s_ddx = L.s_ddx;
+  T *s_rda = L.s_rda, *s_hp = L.s_hp, *s_np = L.s_np, *s_nh = L.s_nh, *s_ndz = L.s_ndz;
   stage_region_state<T, TI, TJ, false>(g, io, b, s_h, s_u, s_v, nullptr);
   for (int e = tid; e < S::C; e += kTileThreads) {
     const int a = e / TJ, q = e % TJ;
@@ -698,58 +718,77 @@ __device__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, 
 // io.h_out must hold the new h of every face (interior) and io.fx / io.fy the
 // face cache of this stage, both from phase H.
 template <typename T, int TI, int TJ>
-__device__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
+struct LayoutUV {
   using S = TileShape<TI, TJ>;
-  constexpr int RJ = S::RJ;
-  const int m = g.m, n = g.n, f = b.f, tid = threadIdx.x;
-  T* s_g = sm;              // cells [C][4] gct (16-byte aligned for cp.async)
-  T* s_s = s_g + 4 * S::C;  // cells: sina
-  T* s_rda = s_s + S::C;
-  T* s_rdx = s_rda + S::C;
-  T* s_rdy = s_rdx + S::C;
-  T* s_af = s_rdy + S::C;
-  T* s_up = s_af + S::C;
-  T* s_vp = s_up + S::C;
-  T* s_u = s_vp + S::C;     // region: raw u, v, new h (then the blended h), stage h
-  T* s_v = s_u + S::R;
-  T* s_hn = s_v + S::R;
-  T* s_h = s_hn + S::R;
-  T* s_xc = s_h + S::R;     // x faces [TI+1][TJ]: cache (3), kinetic energy, tangential v, c_dy
-  T* s_ku = s_xc + 3 * S::FX;
-  T* s_vx = s_ku + S::FX;
-  T* s_cdy = s_vx + S::FX;
-  T* s_yc = s_cdy + S::FX;  // y faces [TI][TJ+1]: cache (3), kinetic energy, tangential u, d_dx
-  T* s_kv = s_yc + 3 * S::FY;
-  T* s_uy = s_kv + S::FY;
-  T* s_ddx = s_uy + S::FY;
-  const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
+  T *s_g, *s_s, *s_rda, *s_rdx, *s_rdy, *s_af, *s_up, *s_vp, *s_u, *s_v, *s_hn, *s_h, *s_xc, *s_ku, *s_vx,
+      *s_cdy, *s_yc, *s_kv, *s_uy, *s_ddx;
+  __device__ __forceinline__ explicit LayoutUV(T* sm) {
+    s_g = sm;              // cells [C][4] gct (16-byte aligned for cp.async)
+    s_s = s_g + 4 * S::C;  // cells: sina
+    s_rda = s_s + S::C;
+    s_rdx = s_rda + S::C;
+    s_rdy = s_rdx + S::C;
+    s_af = s_rdy + S::C;
+    s_up = s_af + S::C;
+    s_vp = s_up + S::C;
+    s_u = s_vp + S::C;     // region: raw u, v, new h (then the blended h), stage h
+    s_v = s_u + S::R;
+    s_hn = s_v + S::R;
+    s_h = s_hn + S::R;
+    s_xc = s_h + S::R;     // x faces [TI+1][TJ]: cache (3), kinetic energy, tangential v, c_dy
+    s_ku = s_xc + 3 * S::FX;
+    s_vx = s_ku + S::FX;
+    s_cdy = s_vx + S::FX;
+    s_yc = s_cdy + S::FX;  // y faces [TI][TJ+1]: cache (3), kinetic energy, tangential u, d_dx
+    s_kv = s_yc + 3 * S::FY;
+    s_uy = s_kv + S::FY;
+    s_ddx = s_uy + S::FY;
+  }
+};
 
-  // constants (before the dependency on phase H)
+// Phase UV prologue: cell and face constants (cp.async) and the halo-gather descriptors.
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                            Gather<T, TI, TJ, true>& gat, int* cnt, int& P) {
+  using S = TileShape<TI, TJ>;
+  const LayoutUV<T, TI, TJ> L(sm);
+  const int m = g.m, f = b.f, tid = threadIdx.x;
   for (int e = tid; e < S::C; e += kTileThreads) {
     const int a = e / TJ, q = e % TJ;
     if (a >= b.ni || q >= b.nj) continue;
     const long o = cell(f, b.i0 + a, b.j0 + q, m);
-    cp_async_mat(s_g + 4 * e, g.gct + 4 * o);
-    cp_async_t(s_s + e, g.sina + o);
-    cp_async_t(s_rda + e, g.rda + o);
-    cp_async_t(s_rdx + e, g.rdx + o);
-    cp_async_t(s_rdy + e, g.rdy + o);
-    cp_async_t(s_af + e, g.a_f + o);
+    cp_async_mat(L.s_g + 4 * e, g.gct + 4 * o);
+    cp_async_t(L.s_s + e, g.sina + o);
+    cp_async_t(L.s_rda + e, g.rda + o);
+    cp_async_t(L.s_rdx + e, g.rdx + o);
+    cp_async_t(L.s_rdy + e, g.rdy + o);
+    cp_async_t(L.s_af + e, g.a_f + o);
   }
   for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
     if (e < S::FX) {
       const int a = e / TJ, q = e % TJ;
-      if (a <= b.ni && q < b.nj) cp_async_t(s_cdy + e, g.c_dy + cell(f, b.i0 + a, b.j0 + q, m));
+      if (a <= b.ni && q < b.nj) cp_async_t(L.s_cdy + e, g.c_dy + cell(f, b.i0 + a, b.j0 + q, m));
     } else {
       const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
-      if (a < b.ni && q <= b.nj) cp_async_t(s_ddx + e2, g.d_dx + cell(f, b.i0 + a, b.j0 + q, m));
+      if (a < b.ni && q <= b.nj) cp_async_t(L.s_ddx + e2, g.d_dx + cell(f, b.i0 + a, b.j0 + q, m));
     }
   }
-  int cnt[4];
-  const int P = edge_count(b, m, cnt);
-  Gather<T, TI, TJ, true> gat;
+  P = edge_count(b, m, cnt);
   if (P > 0) gat.descriptors(g, io, b, cnt, P);
-  wait_prior_grid();
+}
+
+template <typename T, int TI, int TJ>
+__device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                             Gather<T, TI, TJ, true>& gat, const int* cnt, int P) {
+  using S = TileShape<TI, TJ>;
+  constexpr int RJ = S::RJ;
+  const int m = g.m, n = g.n, f = b.f, tid = threadIdx.x;
+  const LayoutUV<T, TI, TJ> L(sm);
+  T *s_g = L.s_g, *s_s = L.s_s, *s_rda = L.s_rda, *s_rdx = L.s_rdx, *s_rdy = L.s_rdy, *s_af = L.s_af;
+  T *s_up = L.s_up, *s_vp = L.s_vp, *s_u = L.s_u, *s_v = L.s_v, *s_hn = L.s_hn, *s_h = L.s_h;
+  T *s_xc = L.s_xc, *s_ku = L.s_ku, *s_vx = L.s_vx, *s_cdy = L.s_cdy, *s_yc = L.s_yc, *s_kv = L.s_kv;
+  T *s_uy = L.s_uy, *s_ddx = L.s_ddx;
+  const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
 
   // state: region u, v, new h (and h), cells' base velocities, the face cache
   const T* hn_src = (const T*)io.h_out;
@@ -861,37 +900,59 @@ __device__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
   }
 }
 
+// One tile phase with the prologue issued first (the stream/graph kernels).
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
+  Gather<T, TI, TJ, false> gat;
+  int cnt[4], P;
+  tile_h_pro<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+  wait_prior_grid();
+  tile_h_main<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+}
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
+  Gather<T, TI, TJ, true> gat;
+  int cnt[4], P;
+  tile_uv_pro<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+  wait_prior_grid();
+  tile_uv_main<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+}
+
 // ---------------------------------------------------------------------------
 // Grid-wide barrier of the persistent round kernel
 // ---------------------------------------------------------------------------
-// Monotone arrival counter: the k-th barrier completes when the counter reaches
-// k * gridDim.x.  Thread 0 of each CTA publishes the CTA's writes (fence), arrives
-// and spins with a bounded number of polls; on timeout it raises
-// kErrBarrierTimeout and every CTA leaves the round at its next barrier.
+// Monotone arrival counter: the k-th barrier completes when the low 31 bits
+// of the counter reach k * gridDim.x.  Thread 0 of each CTA arrives with a
+// release reduction (publishing the CTA's writes, ordered by the preceding
+// __syncthreads) and polls with acquire loads, at most ``limit`` times.  A CTA
+// that gives up raises kErrBarrierTimeout and sets the counter's top bit, which
+// every other CTA sees at its next poll: all CTAs then leave the round.
 // Returns false when the round must stop.
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* err, long long limit) {
   __shared__ int s_ok;
+  constexpr unsigned kAbort = 0x80000000u;
   __syncthreads();
   if (threadIdx.x == 0) {
     ++gen;
     const unsigned target = gen * gridDim.x;
-    __threadfence();
-    atomicAdd(bar, 1u);
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
     long long polls = 0;
     int ok = 1;
     while (true) {
       unsigned seen;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(bar) : "memory");
-      if ((int)(seen - target) >= 0) break;
-      if (++polls > limit) {
-        atomicOr(err, kErrBarrierTimeout);
+      if (seen & kAbort) {
         ok = 0;
         break;
       }
-      __nanosleep(64);
+      if ((int)((seen & ~kAbort) - target) >= 0) break;
+      if (++polls > limit) {
+        atomicOr(err, kErrBarrierTimeout);
+        atomicOr(bar, kAbort);
+        ok = 0;
+        break;
+      }
     }
-    __threadfence();
-    if (ok && *((volatile int*)err) != 0) ok = 0;
     s_ok = ok;
   }
   __syncthreads();

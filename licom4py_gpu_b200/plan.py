@@ -103,14 +103,17 @@ class BtPlan:
         self.set_option(N.BT_OPT_SPIN_LIMIT, polls)
 
     def enable_kernel_timing(self, on: bool = True) -> None:
-        """Persistent mode: bracket every round kernel with CUDA events on its stream."""
+        """Bracket the round kernel (persistent mode) or each phase kernel (stream
+        mode) with CUDA events on its stream; resets the record."""
         self.set_option(N.BT_OPT_KERNEL_TIMING, 1 if on else 0)
 
-    def kernel_time(self) -> Tuple[float, int]:
-        """(total ms, launches) of the timed round kernels since the last read."""
+    KERNELS = {"round": N.BT_KERNEL_ROUND, "phase_h": N.BT_KERNEL_PHASE_H, "phase_uv": N.BT_KERNEL_PHASE_UV}
+
+    def kernel_time(self, kind: str = "round") -> Tuple[float, int]:
+        """(total ms, launches) of the timed kernels of ``kind`` since timing was enabled."""
         ms = ctypes.c_double()
         n = ctypes.c_int()
-        N.check(N.lib().bt_plan_kernel_time(self._h, ctypes.byref(ms), ctypes.byref(n)))
+        N.check(N.lib().bt_plan_kernel_time(self._h, self.KERNELS[kind], ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
 
     @property
