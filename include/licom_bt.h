@@ -182,6 +182,20 @@ int bt_interior_stats(int n, int dtype, const void* field, void* out3, void* str
 int bt_conservation(int n, int dtype, const void* h, const void* u, const void* v, const void* rda,
                     const void* a_c2l, double depth, void* out2, void* stream);
 
+/* bt_round without any allocation, for callers that cannot allocate device
+ * memory (a runtime's custom-call handler given only its operand buffers, a
+ * model driver that reserves its GPU memory up front, a service whose memory
+ * footprint is fixed once it serves).  No counterpart in the reference.
+ * Same arguments and results as bt_round, but no plan: desc is passed directly
+ * and the halo tables are rebuilt on the device each call, stream-ordered.
+ * All scratch lives in one 6 MiB array the library declares statically
+ * (held by every GPU that loads the library until exit): float64 rounds fit up
+ * to N = 96, larger sizes return BT_EINVAL.  The first call on a device sets
+ * up the array's address and must come before any stream capture.  Calls
+ * share the array: calls whose GPU work overlaps race and must be serialised. */
+int bt_round_noalloc(const bt_grid_desc* desc, const bt_state_in* in, const bt_state_out* out, int nbb,
+                     double dtb, int rk, void* stream);
+
 /* Synchronise the plan's work and report a device-side error flag, if set. */
 int bt_check_device_error(bt_plan* plan);
 

@@ -47,6 +47,7 @@ _lib = None
 EXPORTS = ("bt_plan_create", "bt_plan_destroy", "bt_plan_set_tile", "bt_plan_set_mode",
            "bt_plan_set_option", "bt_plan_get_info", "bt_plan_kernel_time", "bt_round",
            "bt_stage", "bt_fill_halo", "bt_edge_average", "bt_check_device_error", "bt_halo_table_host", "bt_interior_stats", "bt_conservation",
+           "bt_round_noalloc",
            "bt_last_error", "bt_version")
 
 
@@ -78,6 +79,8 @@ def lib():
     L.bt_halo_table_host.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
     L.bt_interior_stats.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
     L.bt_conservation.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _vp]
+    L.bt_round_noalloc.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(StateIn), ctypes.POINTER(StateOut),
+                                   ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp]
     L.bt_last_error.argtypes = []
     L.bt_last_error.restype = ctypes.c_char_p
     L.bt_version.argtypes = []

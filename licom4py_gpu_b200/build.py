@@ -32,7 +32,8 @@ CXX = os.environ.get("CXX", shutil.which("g++") or "g++")
 # without FMA contraction so float64 results round like the reference's
 # arithmetic; the float32 precision form keeps FMA.
 CUDA_SOURCES = [("bt_kernels_f64.cu", ["-fmad=false"]), ("bt_kernels_f32.cu", ["-fmad=true"]),
-                ("bt_capi.cu", ["-fmad=false"]), ("bt_reduce.cu", ["-fmad=false"])]
+                ("bt_capi.cu", ["-fmad=false"]), ("bt_reduce.cu", ["-fmad=false"]),
+                ("bt_noalloc.cu", ["-fmad=false"])]
 CUDA_HEADERS = ["bt_common.cuh", "bt_stencil.cuh", "bt_launch.cuh", "bt_kernels.cuh"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
