@@ -38,7 +38,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-B_ALG_WORDS = 41  # algorithmic words per cell-update (both RK stages), see DESIGN.md
+B_ALG_WORDS = 41  # algorithmic words per cell-update over both RK stages (compulsory reads + writes of phase H and UV)
 # Compulsory words per interior cell of each phase kernel, averaged over the two
 # RK2 stages (stage 1 / stage 2): distinct field reads + writes of the kernel's work.
 #   phase H : h, u, v, [h base], dzph_x, dzph_y, gct(4), sina, rda, c_dy, d_dx -> h     14 / 15

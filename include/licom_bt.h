@@ -202,6 +202,51 @@ int bt_check_device_error(bt_plan* plan);
 const char* bt_last_error(void);
 int bt_version(void);
 
+/* ---- Batched rounds: many independent integrations in one launch ----------
+ * No counterpart in the reference, which advances one state per call
+ * (rk_core, schedule.py:170); a batch replaces a loop of such calls over
+ * ensemble members or served requests.  Members may differ in resolution
+ * (one plan per resolution supplies the geometry; several members may share
+ * a plan), in dtb and in substep count: a round advances member k by its own
+ * nbb substeps, members with fewer substeps retire early and the launch's
+ * later phases cover only the members still running.  Each member's result
+ * is the one bt_round gives for the same input (same tile shape and dtype). */
+typedef struct bt_batch bt_batch;
+
+typedef struct bt_member {
+  bt_plan* plan;       /* geometry of the member's resolution; dtype must match the batch */
+  bt_state_in in;      /* as bt_round */
+  bt_state_out out;    /* as bt_round; diag[0] = NULL skips the diagnostics */
+  void* scratch;       /* device buffer of bt_member_scratch_bytes, 256-byte aligned, private to the member */
+  int nbb;             /* substeps of this round (>= 1) */
+  double dtb;
+} bt_member;
+
+/* Device scratch one member needs for RK order rk (stage fields and face caches). */
+int bt_member_scratch_bytes(bt_plan* plan, int rk, unsigned long long* bytes);
+
+/* A batch of dtype BT_F64 / BT_F32 taking up to max_members members per call,
+ * on the current device.  Default mode BT_MODE_PERSISTENT (one cooperative
+ * launch per round: all phases of all members, grid barriers between phases,
+ * halo fills and diagnostics at the end); BT_MODE_STREAM launches one kernel
+ * per phase over all active members instead.  Tile shape default 8 x 32. */
+int bt_batch_create(int dtype, int max_members, bt_batch** out);
+int bt_batch_destroy(bt_batch* batch);
+int bt_batch_set_mode(bt_batch* batch, int mode);
+int bt_batch_set_tile(bt_batch* batch, int ti, int tj);
+/* BT_OPT_MAX_CTAS and BT_OPT_SPIN_LIMIT, as for plans. */
+int bt_batch_set_option(bt_batch* batch, int key, long long value);
+/* BT_INFO_LAST_GRID; -1 for an unknown key. */
+long long bt_batch_get_info(bt_batch* batch, int key);
+
+/* Advance every member by its nbb substeps of RK order rk (2 or 3), stream
+ * ordered.  The member array is read during the call only.  The host may
+ * block when four earlier calls on this batch are still running on the GPU. */
+int bt_batch_round(bt_batch* batch, const bt_member* members, int count, int rk, void* stream);
+
+/* Synchronise the device and report the batch's device error flag, if set. */
+int bt_batch_check_device_error(bt_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,6 +37,11 @@ class StateOut(ctypes.Structure):
     _fields_ = [("h0", _vp), ("ub", _vp), ("vb", _vp), ("diag", _vp * 10)]
 
 
+class Member(ctypes.Structure):
+    _fields_ = [("plan", _vp), ("inp", StateIn), ("out", StateOut), ("scratch", _vp), ("nbb", ctypes.c_int),
+                ("dtb", ctypes.c_double)]
+
+
 class BtError(RuntimeError):
     """A CUDA or device-side failure reported by libbt."""
 
@@ -48,6 +53,9 @@ EXPORTS = ("bt_plan_create", "bt_plan_destroy", "bt_plan_set_tile", "bt_plan_set
            "bt_plan_set_option", "bt_plan_get_info", "bt_plan_kernel_time", "bt_round",
            "bt_stage", "bt_fill_halo", "bt_edge_average", "bt_check_device_error", "bt_halo_table_host", "bt_interior_stats", "bt_conservation",
            "bt_round_noalloc",
+           "bt_member_scratch_bytes", "bt_batch_create", "bt_batch_destroy", "bt_batch_set_mode",
+           "bt_batch_set_tile", "bt_batch_set_option", "bt_batch_get_info", "bt_batch_round",
+           "bt_batch_check_device_error",
            "bt_last_error", "bt_version")
 
 
@@ -81,6 +89,15 @@ def lib():
     L.bt_conservation.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _vp]
     L.bt_round_noalloc.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(StateIn), ctypes.POINTER(StateOut),
                                    ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp]
+    L.bt_member_scratch_bytes.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.bt_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]
+    L.bt_batch_destroy.argtypes = [_vp]
+    L.bt_batch_set_mode.argtypes = [_vp, ctypes.c_int]
+    L.bt_batch_set_tile.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    L.bt_batch_set_option.argtypes = [_vp, ctypes.c_int, ctypes.c_longlong]
+    L.bt_batch_get_info.argtypes = [_vp, ctypes.c_int]
+    L.bt_batch_round.argtypes = [_vp, ctypes.POINTER(Member), ctypes.c_int, ctypes.c_int, _vp]
+    L.bt_batch_check_device_error.argtypes = [_vp]
     L.bt_last_error.argtypes = []
     L.bt_last_error.restype = ctypes.c_char_p
     L.bt_version.argtypes = []
@@ -88,6 +105,7 @@ def lib():
         if name != "bt_last_error":
             getattr(L, name).restype = ctypes.c_int
     L.bt_plan_get_info.restype = ctypes.c_longlong
+    L.bt_batch_get_info.restype = ctypes.c_longlong
     _lib = L
     return L
 

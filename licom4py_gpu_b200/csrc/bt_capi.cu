@@ -8,8 +8,7 @@
 #include <string>
 #include <vector>
 
-#include "bt_launch.cuh"
-#include "licom_bt.h"
+#include "bt_plan.cuh"
 
 using namespace bt;
 
@@ -85,87 +84,6 @@ void band_cell(int d, int c, int k, int m, int* i, int* j) {
 }
 
 }  // namespace
-
-struct bt_plan {
-  int n = 0, m = 0, nh = 0, dtype = BT_F64, device = 0;
-  TileCfg tile{8, 32};
-  int mode = BT_MODE_STREAM;
-  const void* c[17] = {};
-  int route[24] = {};
-  void* d_hsrc = nullptr;  // int2[6*nh]
-  void* d_hw = nullptr;    // T[6*nh*2]
-  void* scratch = nullptr; // Y (3 fields) + Y2 (3 fields) + edge lines
-  size_t field_elems = 0;
-  cudaStream_t cap_stream = nullptr;
-  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-  // graph cache
-  cudaGraphExec_t gexec = nullptr;
-  std::vector<uintptr_t> gkey;
-  // persistent mode: barrier counter + device error flag, options
-  unsigned* d_flags = nullptr;  // [0] barrier counter, [1] error bits
-  int max_ctas = 0;
-  long long spin_limit = 1ll << 24;
-  int last_grid = 0;
-  // optional kernel timing: event pairs on the launch stream around the round
-  // kernel (persistent mode) or each phase kernel (stream mode), with their kind
-  int timing = 0;
-  mutable std::vector<cudaEvent_t> tev;
-  mutable std::vector<int> tkind;
-  mutable size_t tev_used = 0;
-
-  // Record the start event of a timed kernel of the given kind (nullptr if timing is off).
-  cudaError_t time_begin(int kind, cudaStream_t s, cudaEvent_t* stop) const {
-    *stop = nullptr;
-    if (!timing) return cudaSuccess;
-    if (tev_used + 2 > tev.size()) {
-      for (int k = 0; k < 2; ++k) {
-        cudaEvent_t ev;
-        cudaError_t e = cudaEventCreate(&ev);
-        if (e != cudaSuccess) return e;
-        tev.push_back(ev);
-      }
-    }
-    tkind.resize(tev.size() / 2);
-    tkind[tev_used / 2] = kind;
-    cudaEvent_t start = tev[tev_used];
-    *stop = tev[tev_used + 1];
-    tev_used += 2;
-    return cudaEventRecord(start, s);
-  }
-
-  size_t esize() const { return dtype == BT_F64 ? 8 : 4; }
-  // scratch layout: 6 stage fields, edge lines (24 n), face caches x and y (6 (n+1) n 3 each)
-  size_t face_elems() const { return (size_t)6 * (n + 1) * n * 3; }
-  size_t scratch_elems() const { return 6 * field_elems + 24 * (size_t)n + 2 * face_elems(); }
-  void* scratch_field(int k) const { return (char*)scratch + (size_t)k * field_elems * esize(); }
-  void* edge_lines() const { return scratch_field(6); }
-  void* face_x() const { return (char*)edge_lines() + 24 * (size_t)n * esize(); }
-  void* face_y() const { return (char*)face_x() + face_elems() * esize(); }
-
-  template <typename T>
-  Geo<T> geo() const {
-    Geo<T> g;
-    g.n = n;
-    g.m = m;
-    g.nh = nh;
-    g.dzph_x = (const T*)c[0];
-    g.dzph_y = (const T*)c[1];
-    g.rdx = (const T*)c[2];
-    g.rdy = (const T*)c[3];
-    g.a_f = (const T*)c[4];
-    g.c2l = (const T*)c[8];
-    g.l2c = (const T*)c[9];
-    g.gct = (const T*)c[12];
-    g.sina = (const T*)c[13];
-    g.rda = (const T*)c[14];
-    g.c_dy = (const T*)c[15];
-    g.d_dx = (const T*)c[16];
-    g.hsrc = (const int2*)d_hsrc;
-    g.hw = (const T*)d_hw;
-    std::memcpy(g.route, route, sizeof(route));
-    return g;
-  }
-};
 
 namespace {
 
