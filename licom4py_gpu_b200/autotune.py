@@ -109,3 +109,68 @@ def choose_config(n: int, dtype: torch.dtype = torch.float64, consts: Optional[S
     if consts is None:
         return heuristic(n)
     return tune(n, dtype, consts, dev)
+
+
+# ---- batched rounds ----------------------------------------------------------
+BATCH_MODES = ("persistent", "stream")
+BATCH_CTAS = (0, 148, 296)  # persistent grid caps tried (0 = as many CTAs as fit)
+
+
+def _mix_key(specs, dtype: torch.dtype, rk: int, device) -> str:
+    counts: Dict[int, int] = {}
+    for s in specs:
+        counts[s.n] = counts.get(s.n, 0) + 1
+    mix = ",".join(f"C{n}x{c}" for n, c in sorted(counts.items()))
+    return f"{torch.cuda.get_device_name(device)}|batch|{str(dtype).replace('torch.', '')}|rk{rk}|{mix}"
+
+
+def tune_batch(ens, nsub: int = 48, reps: int = 2, modes: Sequence[str] = BATCH_MODES,
+               tiles: Sequence = TILES, ctas: Sequence[int] = BATCH_CTAS) -> dict:
+    """Time batched rounds of the ensemble ``ens`` for every (mode, tile, grid
+    cap) candidate and cache the fastest.  The trial keeps the mix and its
+    retirement pattern at a shorter length: member k runs
+    max(1, nsub * nsub_k / max nsub) substeps."""
+    from .batch import BtBatch
+    longest = max(s.nsub for s in ens.specs)
+    trial = [max(1, round(nsub * s.nsub / longest)) for s in ens.specs]
+    work = sum(6 * s.n * s.n * k for s, k in zip(ens.specs, trial))
+    results = []
+    for mode in modes:
+        for tile in tiles:
+            for cap in (ctas if mode == "persistent" else (0,)):
+                b = BtBatch(ens.dtype, max_members=len(ens.specs), device=ens.device, mode=mode, tile=tile)
+                try:
+                    b.set_max_ctas(cap)
+                    times = []
+                    for r in range(reps + 1):
+                        mem = ens.members()
+                        for m, k in zip(mem, trial):
+                            m.remaining = k
+                        torch.cuda.synchronize(ens.device)
+                        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        a.record()
+                        b.advance(mem)
+                        z.record()
+                        torch.cuda.synchronize(ens.device)
+                        if r > 0:
+                            times.append(a.elapsed_time(z))
+                    b.check_device_error()
+                    ms = min(times)
+                    results.append({"mode": mode, "tile": list(tile), "max_ctas": cap, "ms": ms,
+                                    "cell_updates_per_s": work / (ms * 1e-3)})
+                finally:
+                    b.close()
+    best = min(results, key=lambda r: r["ms"])
+    cfg = {"mode": best["mode"], "tile": best["tile"], "max_ctas": best["max_ctas"], "source": "tuned",
+           "trial_substeps": nsub, "candidates": results}
+    _store(_mix_key(ens.specs, ens.dtype, ens.rk, ens.device), cfg)
+    return cfg
+
+
+def choose_batch_config(ens, retune: bool = False) -> dict:
+    """Cached tuned batch config for this mix, else tune it now."""
+    if not retune:
+        cfg = _load_cache().get(_mix_key(ens.specs, ens.dtype, ens.rk, ens.device))
+        if cfg is not None:
+            return cfg
+    return tune_batch(ens)

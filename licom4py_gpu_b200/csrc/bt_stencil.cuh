@@ -189,33 +189,59 @@ __device__ __forceinline__ int yface_side(int j, int m) {
 // ---------------------------------------------------------------------------
 // Tile phases
 // ---------------------------------------------------------------------------
-// A CTA of kTileThreads threads computes one TI x TJ tile of one face.  Its
-// stencil region (the tile plus 3 cells on each side, without the region
-// corners) is staged into shared memory with cp.async, so every global load
-// of the region is in flight at once; halo cells of the region are gathered
-// (two-level chain: descriptor, then sources), the neighbouring face's edge
-// values are recomputed, and per-cell / per-face constants are prefetched into
-// registers, all before the first barrier.
+// A CTA of kTileThreads threads computes one TI x TJ tile of one face.  Thread
+// t works on column q = t % TJ of the tile and on the rows sl, sl + NS, ...
+// (sl = t / TJ, NS = kTileThreads / TJ row slots), so a warp always covers
+// consecutive columns of one row: every global access is a run of
+// consecutive cells and every shared-memory stencil read is conflict-free.
+//
+// The stencil region of a tile is a cross: the tile's columns extended by 3
+// rows on each side (the "vertical bar", read along i by the x faces) and
+// the tile's rows extended by 3 columns on each side (the "horizontal bar",
+// read along j by the y faces).  Each thread loads the state of its own
+// interior region points straight into registers and stores the quantities
+// the stencils read (h and the contravariant velocity normal to the faces
+// that read the point); halo points of the region are gathered by the
+// Gather items from the neighbouring face.  Constants are staged with
+// cp.async in a prologue that does not depend on the state.
 constexpr int kTileThreads = 256;
+
+constexpr int up4(int x) { return (x + 3) & ~3; }  // shared-memory offsets in words, 16-byte aligned
 
 template <int TI, int TJ>
 struct TileShape {
-  static constexpr int RI = TI + 6, RJ = TJ + 6, R = RI * RJ;
-  static constexpr int FX = (TI + 1) * TJ;   // x faces
-  static constexpr int FY = TI * (TJ + 1);   // y faces
+  static_assert(TJ == 16 || TJ == 32, "tile columns must be 16 or 32");
+  static constexpr int RI = TI + 6, RJ = TJ + 6;
+  static constexpr int NS = kTileThreads / TJ;      // row slots
+  static constexpr int VB = RI * TJ;                // vertical-bar points (r * TJ + q)
+  static constexpr int SB = 6 * TI;                 // side points: 3 W + 3 E columns per tile row
+  static constexpr int NP = VB + SB;                // staged region points
+  static constexpr int FX = (TI + 1) * TJ;          // x faces (a * TJ + q)
+  static constexpr int FY = TI * (TJ + 1);          // y faces (r * (TJ + 1) + q)
+  static constexpr int C = TI * TJ;                 // cells (a * TJ + q)
   static constexpr int EW = TI > TJ ? TI : TJ;
-  static constexpr int NE = 4 * EW;          // edge slots: 4 kinds x max(TI, TJ) positions
-  static constexpr int NIT = (R + kTileThreads - 1) / kTileThreads;
-  static constexpr int CIT = (TI * TJ + kTileThreads - 1) / kTileThreads;
-  static constexpr int FIT = (FX + FY + kTileThreads - 1) / kTileThreads;
-  static constexpr int C = TI * TJ;
-  // region: h, u, v, g(4), s, uc, vc [+ hn for UV]; face and cell arrays;
-  // neighbour edge lines (6 contravariant values + 6 h values + depth per slot)
-  static constexpr int kWordsH = 10 * R + 3 * FX + 3 * FY + 2 * C + 13 * NE;
-  // UV: cells g(4), s, rda, rdx, rdy, af, up, vp; region u, v, hn, h; faces:
-  // cache (3) + kinetic energy + tangential + c_dy / d_dx
-  static constexpr int kWordsUV = 11 * C + 4 * R + 6 * FX + 6 * FY;
-  static constexpr int MI = 4;               // gather items per thread handled in the two-sweep path
+  static constexpr int NE = 4 * EW;                 // edge slots: 4 kinds x max(TI, TJ) positions
+  static constexpr int KV = (RI + NS - 1) / NS;     // row iterations over the vertical bar
+  static constexpr int KX = (TI + 1 + NS - 1) / NS; // over x-face rows
+  static constexpr int KC = (TI + NS - 1) / NS;     // over tile rows
+  static constexpr int MI = 4;                      // gather items per thread handled in the two-sweep path
+  // phase H (words): s_h [RI][RJ], s_uc [VB], s_vc [TI][RJ], s_g [NP][4], s_sn [NP],
+  // s_dzx/s_cdy [FX], s_dzy/s_ddx [FY], s_rda [C], neighbour lines; s_P [FX] and
+  // s_Q [FY] alias s_g (dead once the region is staged)
+  static constexpr int hH = 0, hUC = up4(hH + RI * RJ), hVC = up4(hUC + VB), hG = up4(hVC + TI * RJ),
+                       hSN = up4(hG + 4 * NP), hDZX = up4(hSN + NP), hCDY = up4(hDZX + FX),
+                       hDZY = up4(hCDY + FX), hDDX = up4(hDZY + FY), hRDA = up4(hDDX + FY),
+                       hNP = up4(hRDA + C), hNH = hNP + 6 * NE, hNDZ = hNH + 6 * NE, kWordsH = up4(hNDZ + NE);
+  static constexpr int hP = hG, hQ = hG + FX;
+  static_assert(FX + FY <= 4 * NP, "face fluxes must fit in the metric block they alias");
+  // phase UV (words): s_v [VB], s_u [TI][RJ], s_hn [RI][RJ], cells g [C][4], sina,
+  // rda, rdx, rdy, a_f; x faces cache [3][FX], c_dy, kinetic energy, v_t * c_dy;
+  // y faces cache [3][FY], d_dx, kinetic energy, u_t * d_dx
+  static constexpr int uV = 0, uU = up4(uV + VB), uHN = up4(uU + TI * RJ), uG = up4(uHN + RI * RJ),
+                       uSN = up4(uG + 4 * C), uRDA = uSN + C, uRDX = uRDA + C, uRDY = uRDX + C, uAF = uRDY + C,
+                       uXC = up4(uAF + C), uCDY = up4(uXC + 3 * FX), uKU = up4(uCDY + FX), uVX = up4(uKU + FX),
+                       uYC = up4(uVX + FX), uDDX = up4(uYC + 3 * FY), uKV = up4(uDDX + FY), uUY = up4(uKV + FY),
+                       kWordsUV = up4(uUY + FY);
 };
 
 struct TileBox {
@@ -235,12 +261,8 @@ __device__ __forceinline__ TileBox tile_box(const Tiling& t, int n, int tile) {
   return b;
 }
 
-// Region point (r, c) of a tile's smem block is needed when it lies in the
-// tile's rows or columns, extended by 3 along the other axis (no region corners).
-__device__ __forceinline__ bool region_needed(int r, int c, int ni, int nj) {
-  const bool rin = r >= kHalo && r < kHalo + ni, cin = c >= kHalo && c < kHalo + nj;
-  return (rin && c < nj + 6) || (cin && r < ni + 6);
-}
+// 32-bit offset of cell (i, j) of face f (fields of up to 2^31 elements).
+__device__ __forceinline__ int cell32(int f, int i, int j, int m) { return (f * m + i) * m + j; }
 
 // ---- asynchronous global -> shared copies ---------------------------------
 template <int BYTES>
@@ -330,9 +352,11 @@ __device__ __forceinline__ EdgeItem edge_item(const TileBox& b, const int* cnt, 
 }
 
 // Work items of a tile that touches face edges, spread over the whole CTA:
-//   item t < 3P:  halo cell at depth t % 3 outside edge position t / 3 of the
-//                 tile (its h, u, v when the stored halo is not valid, and the
-//                 new h in phase UV) -- a gather from the neighbouring face;
+//   item t < 3P:  halo point at depth t % 3 outside edge position t / 3 of the
+//                 tile: its h and normal contravariant velocity (phase H), or
+//                 its raw tangential-reading velocity and new h (phase UV) --
+//                 read directly when the stored halo is valid, else gathered
+//                 from the neighbouring face;
 //   item t >= 3P: point q = (t - 3P) % 6 of the neighbour's 6-point line normal
 //                 to the shared edge at position (t - 3P) / 6: its contravariant
 //                 normal velocity (and h for the mass-flux average).
@@ -341,12 +365,14 @@ __device__ __forceinline__ EdgeItem edge_item(const TileBox& b, const int* cnt, 
 // two L2 round trips instead of one chain per point.
 struct ItemCell {
   int f, i, j;      // cell whose value the item needs
-  int slot;         // region index (region items) or edge slot*6 + q (line items)
+  int kind;         // edge kind 0..3 (S, N, W, E)
+  int r, c;         // region row / column (region items)
+  int slot;         // line item: edge slot * 6 + q
   int line, y, q;   // line item: 1, normal axis (1 = y), point index
 };
 
 __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt, int P, int t, int m, int n,
-                                                const int* route, int RJ, int EW) {
+                                                const int* route, int EW) {
   ItemCell c;
   if (t < 3 * P) {
     const EdgeItem e = edge_item(b, cnt, t / 3);
@@ -361,7 +387,10 @@ __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt
     c.f = b.f;
     c.i = b.i0 - kHalo + r;
     c.j = b.j0 - kHalo + cc;
-    c.slot = r * RJ + cc;
+    c.kind = e.kind;
+    c.r = r;
+    c.c = cc;
+    c.slot = 0;
     c.line = 0;
     c.y = 0;
     c.q = 0;
@@ -374,6 +403,9 @@ __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt
     const int kk = route_rev(r) ? n - 1 - e.k : e.k;
     c.f = route_nb(r);
     edge_point(ns, kk, q, m, c.i, c.j);
+    c.kind = e.kind;
+    c.r = 0;
+    c.c = 0;
     c.slot = (e.kind * EW + e.pos) * 6 + q;
     c.line = 1;
     c.y = (ns == kE || ns == kW);
@@ -381,6 +413,17 @@ __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt
   }
   return c;
 }
+
+// Shared-memory destinations of the gather items of one phase.
+template <typename T>
+struct GatherSink {
+  T* h;    // H: region h [RI][RJ]        UV: blended new h [RI][RJ]
+  T* vb;   // H: s_uc [VB]                UV: raw v [VB]
+  T* hb;   // H: s_vc [TI][RJ]            UV: raw u [TI][RJ]
+  T* np;   // H: neighbour lines (contravariant normal velocity, h, depth)
+  T* nh;
+  T* ndz;
+};
 
 template <typename T, int TI, int TJ, bool UV>
 struct Gather {
@@ -404,7 +447,7 @@ struct Gather {
       const int t = threadIdx.x + k * kTileThreads;
       pl[k] = false;
       if (t < nitems) {
-        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::RJ, S::EW);
+        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::EW);
         if (needs_pull(io, c, g.m)) {
           pd[k] = pull_desc(g, c.f, c.i, c.j);
           pl[k] = true;
@@ -414,19 +457,40 @@ struct Gather {
   }
 
   __device__ __forceinline__ void one(const Geo<T>& g, const StageIO<T>& io, const ItemCell& c, const Pull<T>& p,
-                                      bool pull, T* s_h, T* s_u, T* s_v, T* s_hn, T* s_np, T* s_nh, T* s_ndz) {
-    const bool want_h = !UV && io.last;  // neighbour h for the mass-flux average
+                                      bool pull, const GatherSink<T>& k) {
     const long o = cell(c.f, c.i, c.j, g.m);
     if (!c.line) {
-      if (!io.stored_halo) {  // stored halos are staged by cp.async
-        T u, v;
+      const bool vert = c.kind < 2;  // S/N halo rows belong to the vertical bar
+      const bool direct = io.stored_halo;
+      T u, v;
+      if (direct) {
+        u = io.u[o];
+        v = io.v[o];
+      } else {
         pull_v(p, g, io.u, io.v, o, u, v);
-        s_h[c.slot] = pull_s(p, io.h);
-        s_u[c.slot] = u;
-        s_v[c.slot] = v;
       }
-      if (UV) s_hn[c.slot] = pull_s(p, (const T*)io.h_out);
+      if (!UV) {
+        k.h[c.r * S::RJ + c.c] = direct ? io.h[o] : pull_s(p, io.h);
+        const T* G = g.gct + 4 * o;
+        const T sn = g.sina[o];
+        if (vert)
+          k.vb[c.r * TJ + (c.c - kHalo)] = (G[0] * u + G[1] * v) * sn;  // remap.py:34-39
+        else
+          k.hb[(c.r - kHalo) * S::RJ + c.c] = (G[2] * u + G[3] * v) * sn;
+      } else {
+        T hn = pull_s(p, (const T*)io.h_out);
+        if (io.beta != T(0.0)) {
+          const T h = direct ? io.h[o] : pull_s(p, io.h);
+          hn = (T(1.0) - io.beta) * hn + io.beta * h;  // fb_scheme, barotr_pure.py:52-54
+        }
+        k.h[c.r * S::RJ + c.c] = hn;
+        if (vert)
+          k.vb[c.r * TJ + (c.c - kHalo)] = v;
+        else
+          k.hb[(c.r - kHalo) * S::RJ + c.c] = u;
+      }
     } else {
+      const bool want_h = !UV && io.last;  // neighbour h for the mass-flux average
       T u, v, h = T(0.0);
       if (pull) {
         pull_v(p, g, io.u, io.v, o, u, v);
@@ -436,33 +500,33 @@ struct Gather {
         v = io.v[o];
         if (want_h) h = io.h[o];
       }
-      s_np[c.slot] = contra(g, o, u, v, c.y);
+      k.np[c.slot] = contra(g, o, u, v, c.y);
       if (want_h) {
-        s_nh[c.slot] = h;
-        if (c.q == 3) s_ndz[c.slot / 6] = c.y ? g.dzph_y[o] : g.dzph_x[o];
+        k.nh[c.slot] = h;
+        if (c.q == 3) k.ndz[c.slot / 6] = c.y ? g.dzph_y[o] : g.dzph_x[o];
       }
     }
   }
 
   // sweep 2: sources (state, after the grid dependency) and the items' values
   __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, const int* cnt,
-                                          int P, T* s_h, T* s_u, T* s_v, T* s_hn, T* s_np, T* s_nh, T* s_ndz) {
+                                          int P, const GatherSink<T>& k) {
     const int nitems = kPerPos * P;
 #pragma unroll
-    for (int k = 0; k < S::MI; ++k) {
-      const int t = threadIdx.x + k * kTileThreads;
+    for (int q = 0; q < S::MI; ++q) {
+      const int t = threadIdx.x + q * kTileThreads;
       if (t < nitems) {
-        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::RJ, S::EW);
-        one(g, io, c, pd[k], pl[k], s_h, s_u, s_v, s_hn, s_np, s_nh, s_ndz);
+        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::EW);
+        one(g, io, c, pd[q], pl[q], k);
       }
     }
     // items beyond MI per thread (only tiles spanning several face edges of tiny faces)
     for (int t = threadIdx.x + S::MI * kTileThreads; t < nitems; t += kTileThreads) {
-      const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::RJ, S::EW);
+      const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::EW);
       const bool pull = needs_pull(io, c, g.m);
       Pull<T> p;
       if (pull) p = pull_desc(g, c.f, c.i, c.j);
-      one(g, io, c, p, pull, s_h, s_u, s_v, s_hn, s_np, s_nh, s_ndz);
+      one(g, io, c, p, pull, k);
     }
   }
 };
@@ -479,111 +543,70 @@ __device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol
 // Allow the next kernel of the stream to start its prologue.
 __device__ __forceinline__ void release_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 
-// Constants of the tile's faces and cells, staged by cp.async before the
-// state: depth and c_dy on x faces, depth and d_dx on y faces, and per cell
-// rda (+ rdx, rdy, a_f for phase UV).
-template <typename T, int TI, int TJ, bool UV>
-__device__ __forceinline__ void stage_consts(const Geo<T>& g, const TileBox& b, T* s_dzx, T* s_cdy, T* s_dzy,
-                                             T* s_ddx, T* s_rda, T* s_rdx, T* s_rdy, T* s_af) {
-  using S = TileShape<TI, TJ>;
-  const int m = g.m, f = b.f, tid = threadIdx.x;
-  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
-    if (e < S::FX) {
-      const int a = e / TJ, q = e % TJ;
-      if (a > b.ni || q >= b.nj) continue;
-      const long o = cell(f, b.i0 + a, b.j0 + q, m);
-      cp_async_t(s_dzx + e, g.dzph_x + o);
-      cp_async_t(s_cdy + e, g.c_dy + o);
-    } else {
-      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
-      if (a >= b.ni || q > b.nj) continue;
-      const long o = cell(f, b.i0 + a, b.j0 + q, m);
-      cp_async_t(s_dzy + e2, g.dzph_y + o);
-      cp_async_t(s_ddx + e2, g.d_dx + o);
-    }
-  }
-  for (int e = tid; e < S::C; e += kTileThreads) {
-    const int a = e / TJ, q = e % TJ;
-    if (a >= b.ni || q >= b.nj) continue;
-    const long o = cell(f, b.i0 + a, b.j0 + q, m);
-    cp_async_t(s_rda + e, g.rda + o);
-    if (UV) {
-      cp_async_t(s_rdx + e, g.rdx + o);
-      cp_async_t(s_rdy + e, g.rdy + o);
-      cp_async_t(s_af + e, g.a_f + o);
+// Celerity sqrt(g (h + dz)) with the 10 m/s floor and the viscosity
+// coefficient 4.9 / celerity (barotr_pure.py:21-33).  float64 keeps IEEE
+// sqrt and division like the reference; the float32 form takes the
+// reciprocal square root once (sqrt = x * rsqrt(x)), with the same floor and
+// NaN propagation.
+template <typename T>
+__device__ __forceinline__ void celerity_coef(T hface, T dz, T& c, T& coef) {
+  if constexpr (sizeof(T) == 8) {
+    c = celerity(hface, dz);
+    coef = T(4.9) / c;
+  } else {
+    const float x = 9.8f * (hface + dz);
+    if (x > 0.0f) {
+      const float r = rsqrtf(x);
+      c = x * r;
+      coef = 4.9f * r;
+      if (c < 10.0f) {
+        c = 10.0f;
+        coef = 0.49f;
+      }
+    } else {  // zero, negative depth or NaN: the exact path
+      c = celerity(hface, dz);
+      coef = 4.9f / c;
     }
   }
 }
 
-// gct and sina of the region (constants).
-template <typename T, int TI, int TJ>
-__device__ __forceinline__ void stage_region_consts(const Geo<T>& g, const TileBox& b, T* s_g, T* s_s) {
-  using S = TileShape<TI, TJ>;
-  constexpr int RJ = S::RJ;
-#pragma unroll
-  for (int it = 0; it < S::NIT; ++it) {
-    const int e = threadIdx.x + it * kTileThreads;
-    if (e >= S::R) break;
-    const int r = e / RJ, c = e - r * RJ;
-    if (!region_needed(r, c, b.ni, b.nj)) continue;
-    const long o = cell(b.f, b.i0 - kHalo + r, b.j0 - kHalo + c, g.m);
-    cp_async_mat(s_g + 4 * e, g.gct + 4 * o);
-    cp_async_t(s_s + e, g.sina + o);
+// Region points a thread stages itself: interior points, and halo points that
+// no gather item covers -- the halo rows (columns) that the region of a tile
+// next to a tile thinner than 3 cells reaches without the tile touching that
+// face edge; those are fetched point by point.
+struct EdgeCover {
+  bool s, n, w, e;  // the tile touches face edge S / N / W / E (its halo points there are gather items)
+  __device__ __forceinline__ EdgeCover(const TileBox& b, int m)
+      : s(b.i0 == kHalo), n(b.i0 + b.ni == m - kHalo), w(b.j0 == kHalo), e(b.j0 + b.nj == m - kHalo) {}
+  __device__ __forceinline__ bool row_staged(int i, int m) const {
+    return !((i < kHalo && s) || (i >= m - kHalo && n));
   }
-}
-
-// State of the region: h, u, v (interior cells, or every cell when the stored
-// halo is valid) and the new h of interior cells when HN.
-template <typename T, int TI, int TJ, bool HN>
-__device__ __forceinline__ void stage_region_state(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
-                                                   T* s_h, T* s_u, T* s_v, T* s_hn) {
-  using S = TileShape<TI, TJ>;
-  constexpr int RJ = S::RJ;
-  const int m = g.m;
-  const T* hn_src = (const T*)io.h_out;
-#pragma unroll
-  for (int it = 0; it < S::NIT; ++it) {
-    const int e = threadIdx.x + it * kTileThreads;
-    if (e >= S::R) break;
-    const int r = e / RJ, c = e - r * RJ;
-    if (!region_needed(r, c, b.ni, b.nj)) continue;
-    const int i = b.i0 - kHalo + r, j = b.j0 - kHalo + c;
-    const long o = cell(b.f, i, j, m);
-    const bool inner = is_interior(i, j, m);
-    if (io.stored_halo || inner) {
-      cp_async_t(s_h + e, io.h + o);
-      cp_async_t(s_u + e, io.u + o);
-      cp_async_t(s_v + e, io.v + o);
-    }
-    if (HN && inner) cp_async_t(s_hn + e, hn_src + o);
+  __device__ __forceinline__ bool col_staged(int j, int m) const {
+    return !((j < kHalo && w) || (j >= m - kHalo && e));
   }
-}
+};
 
-// Shared-memory layout of phase H (offsets in words).
+// ---- phase H ----------------------------------------------------------------
 template <typename T, int TI, int TJ>
 struct LayoutH {
   using S = TileShape<TI, TJ>;
-  T *s_h, *s_u, *s_v, *s_g, *s_s, *s_uc, *s_vc, *s_fu, *s_fv, *s_dzx, *s_cdy, *s_dzy, *s_ddx, *s_rda, *s_hp,
-      *s_np, *s_nh, *s_ndz;
+  T *s_h, *s_uc, *s_vc, *s_g, *s_sn, *s_dzx, *s_cdy, *s_dzy, *s_ddx, *s_rda, *s_P, *s_Q, *s_np, *s_nh, *s_ndz;
   __device__ __forceinline__ explicit LayoutH(T* sm) {
-    s_h = sm;
-    s_u = s_h + S::R;
-    s_v = s_u + S::R;
-    s_g = s_v + S::R;      // [R][4]
-    s_s = s_g + 4 * S::R;
-    s_uc = s_s + S::R;
-    s_vc = s_uc + S::R;
-    s_fu = s_vc + S::R;    // [TI+1][TJ] mass flux on x faces
-    s_fv = s_fu + S::FX;   // [TI][TJ+1] on y faces
-    s_dzx = s_fv + S::FY;  // [TI+1][TJ]
-    s_cdy = s_dzx + S::FX;
-    s_dzy = s_cdy + S::FX; // [TI][TJ+1]
-    s_ddx = s_dzy + S::FY;
-    s_rda = s_ddx + S::FY; // [TI][TJ]
-    s_hp = s_rda + S::C;
-    s_np = s_hp + S::C;    // [NE][6] neighbour line: contravariant normal velocity
-    s_nh = s_np + 6 * S::NE;   // [NE][6] neighbour line: h
-    s_ndz = s_nh + 6 * S::NE;  // [NE] neighbour depth at the edge face
+    s_h = sm + S::hH;
+    s_uc = sm + S::hUC;
+    s_vc = sm + S::hVC;
+    s_g = sm + S::hG;
+    s_sn = sm + S::hSN;
+    s_dzx = sm + S::hDZX;
+    s_cdy = sm + S::hCDY;
+    s_dzy = sm + S::hDZY;
+    s_ddx = sm + S::hDDX;
+    s_rda = sm + S::hRDA;
+    s_P = sm + S::hP;
+    s_Q = sm + S::hQ;
+    s_np = sm + S::hNP;
+    s_nh = sm + S::hNH;
+    s_ndz = sm + S::hNDZ;
   }
 };
 
@@ -593,11 +616,103 @@ struct LayoutH {
 template <typename T, int TI, int TJ>
 __device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
                                            Gather<T, TI, TJ, false>& gat, int* cnt, int& P) {
+  using S = TileShape<TI, TJ>;
   const LayoutH<T, TI, TJ> L(sm);
-  stage_region_consts<T, TI, TJ>(g, b, L.s_g, L.s_s);
-  stage_consts<T, TI, TJ, false>(g, b, L.s_dzx, L.s_cdy, L.s_dzy, L.s_ddx, L.s_rda, nullptr, nullptr, nullptr);
-  P = edge_count(b, g.m, cnt);
+  const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
+  // region metric (halo points of edge tiles are also read by the gather items, from global memory)
+  if (q < b.nj) {
+    const int o0 = cell32(b.f, b.i0 - kHalo, b.j0 + q, m);
+#pragma unroll
+    for (int k = 0; k < S::KV; ++k) {
+      const int r = sl + k * S::NS;
+      if (r < b.ni + 6) {
+        const int o = o0 + r * m, p = r * TJ + q;
+        cp_async_mat(L.s_g + 4 * p, g.gct + 4 * (long)o);
+        cp_async_t(L.s_sn + p, g.sina + o);
+      }
+    }
+  }
+  if (threadIdx.x < 6 * b.ni) {
+    const int t = threadIdx.x, r = t / 6, c = t - 6 * r, cc = c < 3 ? c : b.nj + c;
+    const int o = cell32(b.f, b.i0 + r, b.j0 - kHalo + cc, m), p = S::VB + t;
+    cp_async_mat(L.s_g + 4 * p, g.gct + 4 * (long)o);
+    cp_async_t(L.s_sn + p, g.sina + o);
+  }
+  // face and cell constants
+  if (q < b.nj) {
+    const int o0 = cell32(b.f, b.i0, b.j0 + q, m);
+#pragma unroll
+    for (int k = 0; k < S::KX; ++k) {
+      const int a = sl + k * S::NS;
+      if (a <= b.ni) {
+        cp_async_t(L.s_dzx + a * TJ + q, g.dzph_x + o0 + a * m);
+        cp_async_t(L.s_cdy + a * TJ + q, g.c_dy + o0 + a * m);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < S::KC; ++k) {
+      const int a = sl + k * S::NS;
+      if (a < b.ni) cp_async_t(L.s_rda + a * TJ + q, g.rda + o0 + a * m);
+    }
+  }
+  if (q <= b.nj) {
+    const int o0 = cell32(b.f, b.i0, b.j0 + q, m);
+#pragma unroll
+    for (int k = 0; k < S::KC; ++k) {
+      const int r = sl + k * S::NS;
+      if (r < b.ni) {
+        cp_async_t(L.s_dzy + r * (TJ + 1) + q, g.dzph_y + o0 + r * m);
+        cp_async_t(L.s_ddx + r * (TJ + 1) + q, g.d_dx + o0 + r * m);
+      }
+    }
+  }
+  if (b.nj == TJ && threadIdx.x < b.ni) {  // the last y-face column of full-width tiles
+    const int r = threadIdx.x, o = cell32(b.f, b.i0 + r, b.j0 + TJ, m);
+    cp_async_t(L.s_dzy + r * (TJ + 1) + TJ, g.dzph_y + o);
+    cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + o);
+  }
+  P = edge_count(b, m, cnt);
   if (P > 0) gat.descriptors(g, io, b, cnt, P);
+}
+
+// Phase H of one x face or y face: C-grid normal velocity (remap.py:41-55)
+// and its edge average (communication.py:504-570), upwind mass flux with the
+// celerity-based velocity viscosity (barotr_pure.py:21-49) and its edge
+// average on the last stage, and the face cache of phase UV.
+// ph / pu: the 6 h / contravariant values along the face normal (strides sh / su).
+template <typename T>
+__device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, const T* pu, int su, int side,
+                                    int slot, T dz, const T* s_np, const T* s_nh, const T* s_ndz, T* fc,
+                                    long pstride) {
+  T hh[6], uu[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    hh[k] = ph[k * sh];
+    uu[k] = pu[k * su];
+  }
+  const T ue = rplus(uu, 1), uw = rminus(uu + 1, 1);
+  T bc = T(0.5) * (ue + uw);
+  if (side >= 0) bc = (bc + line_raw(s_np + 6 * slot)) / T(2.0);
+  const T he = rplus(hh, 1), hw = rminus(hh + 1, 1);
+  T cc, coef;
+  celerity_coef(mid6(hh, 1), dz, cc, coef);
+  const T vis = bc + coef * (he - hw);
+  T fl = dz * vis + (vis > T(0.0) ? he : hw) * vis;
+  if (io.last && side >= 0) {  // the neighbour's flux at the same edge face (barotr_pure.py:29-49)
+    const T* nh = s_nh + 6 * slot;
+    const T ndz = s_ndz[slot];
+    const T nhe = rplus(nh, 1), nhw = rminus(nh + 1, 1);
+    T nc, ncoef;
+    celerity_coef(mid6(nh, 1), ndz, nc, ncoef);
+    const T nvis = bc + ncoef * (nhe - nhw);
+    fl = (fl + (ndz * nvis + (nvis > T(0.0) ? nhe : nhw) * nvis)) / T(2.0);
+  }
+  if (fc) {  // face cache for phase UV: three planes pstride apart
+    fc[0] = bc;
+    fc[pstride] = vis;
+    fc[2 * pstride] = T(0.5) * cc * (ue - uw);  // celerity viscosity flux, barotr_pure.py:68-69
+  }
+  return fl;
 }
 
 // Phase H of one tile: writes the new h on the tile's interior cells.
@@ -606,143 +721,153 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
                             Gather<T, TI, TJ, false>& gat, const int* cnt, int P) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
-  const int m = g.m, f = b.f, tid = threadIdx.x;
+  static_assert(6 * TI <= kTileThreads, "one side point per thread");
+  const int m = g.m, n = g.n, f = b.f, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
   const LayoutH<T, TI, TJ> L(sm);
-  T* s_h = L.s_h;
-  T *s_u = L.s_u, *s_v = L.s_v, *s_g = L.s_g, *s_s = L.s_s, *s_uc = L.s_uc, *s_vc = L.s_vc;
-  T *s_fu = L.s_fu, *s_fv = L.s_fv, *s_dzx = L.s_dzx, *s_cdy = L.s_cdy, *s_dzy = L.s_dzy, *s_ddx = L.s_ddx;
-  T *s_rda = L.s_rda, *s_hp = L.s_hp, *s_np = L.s_np, *s_nh = L.s_nh, *s_ndz = L.s_ndz;
-  stage_region_state<T, TI, TJ, false>(g, io, b, s_h, s_u, s_v, nullptr);
-  for (int e = tid; e < S::C; e += kTileThreads) {
-    const int a = e / TJ, q = e % TJ;
-    if (a < b.ni && q < b.nj) cp_async_t(s_hp + e, io.hp + cell(f, b.i0 + a, b.j0 + q, m));
+  // state of the thread's interior region points and base h of its cells, into registers
+  T hv[S::KV], uv[S::KV], vv[S::KV], hpc[S::KC];
+  T hs = T(0.0), us = T(0.0), vs = T(0.0);
+  const EdgeCover ec(b, m);
+  const int ov = cell32(f, b.i0 - kHalo, b.j0 + q, m);
+#pragma unroll
+  for (int k = 0; k < S::KV; ++k) {
+    const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
+    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
+      if (i >= kHalo && i < m - kHalo) {
+        const int o = ov + r * m;
+        hv[k] = io.h[o];
+        uv[k] = io.u[o];
+        vv[k] = io.v[o];
+      } else {
+        hv[k] = fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
+        fetch_v(io.u, io.v, g, f, i, b.j0 + q, io.stored_halo, uv[k], vv[k]);
+      }
+    }
   }
-  if (P > 0) gat.sources(g, io, b, cnt, P, s_h, s_u, s_v, nullptr, s_np, s_nh, s_ndz);
+  const int t6 = threadIdx.x;
+  const int sr = t6 / 6, sc = t6 - 6 * sr, scc = sc < 3 ? sc : b.nj + sc, sj = b.j0 - kHalo + scc;
+  const bool side_pt = t6 < 6 * b.ni && ec.col_staged(sj, m);
+  if (side_pt) {
+    if (sj >= kHalo && sj < m - kHalo) {
+      const int o = cell32(f, b.i0 + sr, sj, m);
+      hs = io.h[o];
+      us = io.u[o];
+      vs = io.v[o];
+    } else {
+      hs = fetch_s(io.h, g, f, b.i0 + sr, sj, io.stored_halo);
+      fetch_v(io.u, io.v, g, f, b.i0 + sr, sj, io.stored_halo, us, vs);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < S::KC; ++k) {
+    const int a = sl + k * S::NS;
+    if (q < b.nj && a < b.ni) hpc[k] = io.hp[ov + (a + kHalo) * m];
+  }
+  if (P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_h, L.s_uc, L.s_vc, L.s_np, L.s_nh, L.s_ndz});
   cp_async_wait_all();
   __syncthreads();
 
-  // contravariant velocities on the region (remap.py:34-39)
+  // h and contravariant velocities of the region (remap.py:34-39)
 #pragma unroll
-  for (int it = 0; it < S::NIT; ++it) {
-    const int e = tid + it * kTileThreads;
-    if (e >= S::R) break;
-    const int r = e / RJ, c = e - r * RJ;
-    if (!region_needed(r, c, b.ni, b.nj)) continue;
-    const T* G = s_g + 4 * e;
-    const T u = s_u[e], v = s_v[e], sn = s_s[e];
-    s_uc[e] = (G[0] * u + G[1] * v) * sn;
-    s_vc[e] = (G[2] * u + G[3] * v) * sn;
+  for (int k = 0; k < S::KV; ++k) {
+    const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
+    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
+      const int p = r * TJ + q;
+      const T* G = L.s_g + 4 * p;
+      const T sn = L.s_sn[p], u = uv[k], v = vv[k];
+      L.s_h[r * RJ + q + kHalo] = hv[k];
+      L.s_uc[p] = (G[0] * u + G[1] * v) * sn;
+      if (r >= kHalo && r < b.ni + kHalo) L.s_vc[(r - kHalo) * RJ + q + kHalo] = (G[2] * u + G[3] * v) * sn;
+    }
+  }
+  if (side_pt) {
+    const T* G = L.s_g + 4 * (S::VB + t6);
+    const T sn = L.s_sn[S::VB + t6];
+    L.s_h[(sr + kHalo) * RJ + scc] = hs;
+    L.s_vc[sr * RJ + scc] = (G[2] * us + G[3] * vs) * sn;
   }
   __syncthreads();
 
-  // faces: x faces i = i0..i0+ni on the tile's columns, then y faces j = j0..j0+nj on its rows
-  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
-    const bool xf = e < S::FX;
-    int a, q, stride, base, side, kind, pos, fi;
-    if (xf) {
-      a = e / TJ;
-      q = e % TJ;
-      if (a > b.ni || q >= b.nj) continue;
-      stride = RJ;
-      base = a * RJ + (q + kHalo);
-      side = xface_side(b.i0 + a, m);
-      kind = side == kS ? 0 : 1;
-      pos = q;
-      fi = e;
+  // faces; their fluxes (times c_dy / d_dx) alias the metric block, no longer read
+  const long PF = 6L * (n + 1) * n;  // plane size of both face caches
+  if (q < b.nj) {
+#pragma unroll
+    for (int k = 0; k < S::KX; ++k) {
+      const int a = sl + k * S::NS;
+      if (a <= b.ni) {
+        const int side = (a == 0 && b.i0 == kHalo) ? kS : ((a == b.ni && b.i0 + b.ni == m - kHalo) ? kN : -1);
+        const int e = a * TJ + q;
+        T* fc = (a < b.ni || side == kN)
+                    ? io.fx + (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q))
+                    : nullptr;
+        const T fl = face_h<T>(io, L.s_h + a * RJ + q + kHalo, RJ, L.s_uc + a * TJ + q, TJ, side,
+                               (side == kS ? 0 : 1) * S::EW + q, L.s_dzx[e], L.s_np, L.s_nh, L.s_ndz, fc, PF);
+        L.s_P[e] = fl * L.s_cdy[e];
+      }
+    }
+  }
+  // y faces: (r, qq) with qq = q, plus qq = TJ for full-width tiles (threads < ni)
+#pragma unroll
+  for (int k = 0; k <= S::KC; ++k) {
+    int r, qq;
+    if (k < S::KC) {
+      r = sl + k * S::NS;
+      qq = q;
+      if (r >= b.ni || q > b.nj) continue;
     } else {
-      fi = e - S::FX;
-      a = fi / (TJ + 1);
-      q = fi % (TJ + 1);
-      if (a >= b.ni || q > b.nj) continue;
-      stride = 1;
-      base = (a + kHalo) * RJ + q;
-      side = yface_side(b.j0 + q, m);
-      kind = side == kW ? 2 : 3;
-      pos = a;
+      r = threadIdx.x;
+      qq = TJ;
+      if (b.nj != TJ || r >= b.ni) continue;
     }
-    const T* ph = s_h + base;
-    const T* pu = (xf ? s_uc : s_vc) + base;
-    const T ue = rplus(pu, stride), uw = rminus(pu + stride, stride);
-    T bc = T(0.5) * (ue + uw);
-    const int slot = kind * S::EW + pos;
-    if (side >= 0) bc = (bc + line_raw(s_np + 6 * slot)) / T(2.0);
-    const T dz = xf ? s_dzx[fi] : s_dzy[fi];
-    const T he = rplus(ph, stride), hw = rminus(ph + stride, stride);
-    const T cc = celerity(mid6(ph, stride), dz);
-    const T vis = bc + (T(4.9) / cc) * (he - hw);
-    T fl = dz * vis + (vis > T(0.0) ? he : hw) * vis;
-    if (io.last && side >= 0) {  // the neighbour's flux at the same edge face (barotr_pure.py:29-49)
-      const T* nh = s_nh + 6 * slot;
-      const T ndz = s_ndz[slot];
-      const T nhe = rplus(nh, 1), nhw = rminus(nh + 1, 1);
-      const T nc = celerity(mid6(nh, 1), ndz);
-      const T nvis = bc + (T(4.9) / nc) * (nhe - nhw);
-      fl = (fl + (ndz * nvis + (nvis > T(0.0) ? nhe : nhw) * nvis)) / T(2.0);
-    }
-    // face cache for phase UV: each face is written by the one tile that owns it
-    const int n = g.n;
-    T* fc;
-    if (xf) {
-      s_fu[fi] = fl;
-      fc = (a < b.ni || b.i0 + b.ni == m - kHalo)
-               ? io.fx + 3 * (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q))
-               : nullptr;
-    } else {
-      s_fv[fi] = fl;
-      fc = (q < b.nj || b.j0 + b.nj == m - kHalo)
-               ? io.fy + 3 * (((long)f * n + (b.i0 - kHalo + a)) * (n + 1) + (b.j0 - kHalo + q))
-               : nullptr;
-    }
-    if (fc) {
-      fc[0] = bc;
-      fc[1] = vis;
-      fc[2] = T(0.5) * cc * (ue - uw);   // celerity viscosity flux, barotr_pure.py:68-69
-    }
+    const int side = (qq == 0 && b.j0 == kHalo) ? kW : ((qq == b.nj && b.j0 + b.nj == m - kHalo) ? kE : -1);
+    const int e = r * (TJ + 1) + qq;
+    T* fc = (qq < b.nj || side == kE)
+                ? io.fy + (((long)f * n + (b.i0 - kHalo + r)) * (n + 1) + (b.j0 - kHalo + qq))
+                : nullptr;
+    const T fl = face_h<T>(io, L.s_h + (r + kHalo) * RJ + qq, 1, L.s_vc + r * RJ + qq, 1, side,
+                           (side == kW ? 2 : 3) * S::EW + r, L.s_dzy[e], L.s_np, L.s_nh, L.s_ndz, fc, PF);
+    L.s_Q[e] = fl * L.s_ddx[e];
   }
   __syncthreads();
 
   // cells: divergence (agrid.py:43-53) and the h update (barotr_pure.py:119-120)
-  for (int e = tid; e < S::C; e += kTileThreads) {
-    const int a = e / TJ, q = e % TJ;
-    if (a >= b.ni || q >= b.nj) continue;
-    const long o = cell(f, b.i0 + a, b.j0 + q, m);
-    const int x0 = e, x1 = e + TJ;
-    const int y0 = a * (TJ + 1) + q, y1 = y0 + 1;
-    const T div = s_rda[x0] * (s_fu[x1] * s_cdy[x1] - s_fu[x0] * s_cdy[x0] + s_fv[y1] * s_ddx[y1] -
-                               s_fv[y0] * s_ddx[y0]);
-    io.h_out[o] = s_hp[x0] - div * io.dt;
+  if (q < b.nj) {
+#pragma unroll
+    for (int k = 0; k < S::KC; ++k) {
+      const int a = sl + k * S::NS;
+      if (a < b.ni) {
+        const int x0 = a * TJ + q, y0 = a * (TJ + 1) + q;
+        const T div = L.s_rda[x0] * (L.s_P[x0 + TJ] - L.s_P[x0] + L.s_Q[y0 + 1] - L.s_Q[y0]);
+        io.h_out[ov + (a + kHalo) * m] = hpc[k] - div * io.dt;
+      }
+    }
   }
 }
 
-// Phase UV of one tile: writes the new u, v on the tile's interior cells.
-// io.h_out must hold the new h of every face (interior) and io.fx / io.fy the
-// face cache of this stage, both from phase H.
+// ---- phase UV -----------------------------------------------------------------
 template <typename T, int TI, int TJ>
 struct LayoutUV {
   using S = TileShape<TI, TJ>;
-  T *s_g, *s_s, *s_rda, *s_rdx, *s_rdy, *s_af, *s_up, *s_vp, *s_u, *s_v, *s_hn, *s_h, *s_xc, *s_ku, *s_vx,
-      *s_cdy, *s_yc, *s_kv, *s_uy, *s_ddx;
+  T *s_v, *s_u, *s_hn, *s_g, *s_sn, *s_rda, *s_rdx, *s_rdy, *s_af, *s_xc, *s_cdy, *s_ku, *s_vx, *s_yc, *s_ddx,
+      *s_kv, *s_uy;
   __device__ __forceinline__ explicit LayoutUV(T* sm) {
-    s_g = sm;              // cells [C][4] gct (16-byte aligned for cp.async)
-    s_s = s_g + 4 * S::C;  // cells: sina
-    s_rda = s_s + S::C;
-    s_rdx = s_rda + S::C;
-    s_rdy = s_rdx + S::C;
-    s_af = s_rdy + S::C;
-    s_up = s_af + S::C;
-    s_vp = s_up + S::C;
-    s_u = s_vp + S::C;     // region: raw u, v, new h (then the blended h), stage h
-    s_v = s_u + S::R;
-    s_hn = s_v + S::R;
-    s_h = s_hn + S::R;
-    s_xc = s_h + S::R;     // x faces [TI+1][TJ]: cache (3), kinetic energy, tangential v, c_dy
-    s_ku = s_xc + 3 * S::FX;
-    s_vx = s_ku + S::FX;
-    s_cdy = s_vx + S::FX;
-    s_yc = s_cdy + S::FX;  // y faces [TI][TJ+1]: cache (3), kinetic energy, tangential u, d_dx
-    s_kv = s_yc + 3 * S::FY;
-    s_uy = s_kv + S::FY;
-    s_ddx = s_uy + S::FY;
+    s_v = sm + S::uV;
+    s_u = sm + S::uU;
+    s_hn = sm + S::uHN;
+    s_g = sm + S::uG;
+    s_sn = sm + S::uSN;
+    s_rda = sm + S::uRDA;
+    s_rdx = sm + S::uRDX;
+    s_rdy = sm + S::uRDY;
+    s_af = sm + S::uAF;
+    s_xc = sm + S::uXC;
+    s_cdy = sm + S::uCDY;
+    s_ku = sm + S::uKU;
+    s_vx = sm + S::uVX;
+    s_yc = sm + S::uYC;
+    s_ddx = sm + S::uDDX;
+    s_kv = sm + S::uKV;
+    s_uy = sm + S::uUY;
   }
 };
 
@@ -752,26 +877,38 @@ __device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& i
                                             Gather<T, TI, TJ, true>& gat, int* cnt, int& P) {
   using S = TileShape<TI, TJ>;
   const LayoutUV<T, TI, TJ> L(sm);
-  const int m = g.m, f = b.f, tid = threadIdx.x;
-  for (int e = tid; e < S::C; e += kTileThreads) {
-    const int a = e / TJ, q = e % TJ;
-    if (a >= b.ni || q >= b.nj) continue;
-    const long o = cell(f, b.i0 + a, b.j0 + q, m);
-    cp_async_mat(L.s_g + 4 * e, g.gct + 4 * o);
-    cp_async_t(L.s_s + e, g.sina + o);
-    cp_async_t(L.s_rda + e, g.rda + o);
-    cp_async_t(L.s_rdx + e, g.rdx + o);
-    cp_async_t(L.s_rdy + e, g.rdy + o);
-    cp_async_t(L.s_af + e, g.a_f + o);
-  }
-  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
-    if (e < S::FX) {
-      const int a = e / TJ, q = e % TJ;
-      if (a <= b.ni && q < b.nj) cp_async_t(L.s_cdy + e, g.c_dy + cell(f, b.i0 + a, b.j0 + q, m));
-    } else {
-      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
-      if (a < b.ni && q <= b.nj) cp_async_t(L.s_ddx + e2, g.d_dx + cell(f, b.i0 + a, b.j0 + q, m));
+  const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
+  const int o0 = cell32(b.f, b.i0, b.j0 + q, m);
+  if (q < b.nj) {
+#pragma unroll
+    for (int k = 0; k < S::KC; ++k) {
+      const int a = sl + k * S::NS;
+      if (a < b.ni) {
+        const int o = o0 + a * m, e = a * TJ + q;
+        cp_async_mat(L.s_g + 4 * e, g.gct + 4 * (long)o);
+        cp_async_t(L.s_sn + e, g.sina + o);
+        cp_async_t(L.s_rda + e, g.rda + o);
+        cp_async_t(L.s_rdx + e, g.rdx + o);
+        cp_async_t(L.s_rdy + e, g.rdy + o);
+        cp_async_t(L.s_af + e, g.a_f + o);
+      }
     }
+#pragma unroll
+    for (int k = 0; k < S::KX; ++k) {
+      const int a = sl + k * S::NS;
+      if (a <= b.ni) cp_async_t(L.s_cdy + a * TJ + q, g.c_dy + o0 + a * m);
+    }
+  }
+  if (q <= b.nj) {
+#pragma unroll
+    for (int k = 0; k < S::KC; ++k) {
+      const int r = sl + k * S::NS;
+      if (r < b.ni) cp_async_t(L.s_ddx + r * (TJ + 1) + q, g.d_dx + o0 + r * m);
+    }
+  }
+  if (b.nj == TJ && threadIdx.x < b.ni) {
+    const int r = threadIdx.x;
+    cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + cell32(b.f, b.i0 + r, b.j0 + TJ, m));
   }
   P = edge_count(b, m, cnt);
   if (P > 0) gat.descriptors(g, io, b, cnt, P);
@@ -782,121 +919,194 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
                              Gather<T, TI, TJ, true>& gat, const int* cnt, int P) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
-  const int m = g.m, n = g.n, f = b.f, tid = threadIdx.x;
+  static_assert(6 * TI <= kTileThreads, "one side point per thread");
+  const int m = g.m, n = g.n, f = b.f, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
   const LayoutUV<T, TI, TJ> L(sm);
-  T *s_g = L.s_g, *s_s = L.s_s, *s_rda = L.s_rda, *s_rdx = L.s_rdx, *s_rdy = L.s_rdy, *s_af = L.s_af;
-  T *s_up = L.s_up, *s_vp = L.s_vp, *s_u = L.s_u, *s_v = L.s_v, *s_hn = L.s_hn, *s_h = L.s_h;
-  T *s_xc = L.s_xc, *s_ku = L.s_ku, *s_vx = L.s_vx, *s_cdy = L.s_cdy, *s_yc = L.s_yc, *s_kv = L.s_kv;
-  T *s_uy = L.s_uy, *s_ddx = L.s_ddx;
   const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
-
-  // state: region u, v, new h (and h), cells' base velocities, the face cache
   const T* hn_src = (const T*)io.h_out;
+  const long PF = 6L * (n + 1) * n;
+
+  // face caches of this stage (written by phase H) -> shared memory
+  if (q < b.nj) {
 #pragma unroll
-  for (int it = 0; it < S::NIT; ++it) {
-    const int e = tid + it * kTileThreads;
-    if (e >= S::R) break;
-    const int r = e / RJ, c = e - r * RJ;
-    if (!region_needed(r, c, b.ni, b.nj)) continue;
-    const int i = b.i0 - kHalo + r, j = b.j0 - kHalo + c;
-    const long o = cell(f, i, j, m);
-    const bool inner = is_interior(i, j, m);
-    if (io.stored_halo || inner) {
-      cp_async_t(s_u + e, io.u + o);
-      cp_async_t(s_v + e, io.v + o);
-      if (blend) cp_async_t(s_h + e, io.h + o);
+    for (int k = 0; k < S::KX; ++k) {
+      const int a = sl + k * S::NS;
+      if (a <= b.ni) {
+        const T* src = io.fx + (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q));
+        const int e = a * TJ + q;
+        cp_async_t(L.s_xc + e, src);
+        cp_async_t(L.s_xc + S::FX + e, src + PF);
+        cp_async_t(L.s_xc + 2 * S::FX + e, src + 2 * PF);
+      }
     }
-    if (inner) cp_async_t(s_hn + e, hn_src + o);
   }
-  for (int e = tid; e < S::C; e += kTileThreads) {
-    const int a = e / TJ, q = e % TJ;
-    if (a >= b.ni || q >= b.nj) continue;
-    const long o = cell(f, b.i0 + a, b.j0 + q, m);
-    cp_async_t(s_up + e, io.up + o);
-    cp_async_t(s_vp + e, io.vp + o);
-  }
-  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
-    const T* src;
-    T* dst;
-    if (e < S::FX) {
-      const int a = e / TJ, q = e % TJ;
-      if (a > b.ni || q >= b.nj) continue;
-      src = io.fx + 3 * (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q));
-      dst = s_xc + 3 * e;
+#pragma unroll
+  for (int k = 0; k <= S::KC; ++k) {
+    int r, qq;
+    if (k < S::KC) {
+      r = sl + k * S::NS;
+      qq = q;
+      if (r >= b.ni || q > b.nj) continue;
     } else {
-      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
-      if (a >= b.ni || q > b.nj) continue;
-      src = io.fy + 3 * (((long)f * n + (b.i0 - kHalo + a)) * (n + 1) + (b.j0 - kHalo + q));
-      dst = s_yc + 3 * e2;
+      r = threadIdx.x;
+      qq = TJ;
+      if (b.nj != TJ || r >= b.ni) continue;
     }
-    cp_async_t(dst, src);
-    cp_async_t(dst + 1, src + 1);
-    cp_async_t(dst + 2, src + 2);
+    const T* src = io.fy + (((long)f * n + (b.i0 - kHalo + r)) * (n + 1) + (b.j0 - kHalo + qq));
+    const int e = r * (TJ + 1) + qq;
+    cp_async_t(L.s_yc + e, src);
+    cp_async_t(L.s_yc + S::FY + e, src + PF);
+    cp_async_t(L.s_yc + 2 * S::FY + e, src + 2 * PF);
   }
-  if (P > 0) gat.sources(g, io, b, cnt, P, s_h, s_u, s_v, s_hn, nullptr, nullptr, nullptr);
+
+  // state of the thread's interior region points and base velocities of its cells
+  T hnv[S::KV], vvv[S::KV], uvv[S::KV], upc[S::KC], vpc[S::KC];
+  T hns = T(0.0), us = T(0.0);
+  const EdgeCover ec(b, m);
+  const int ov = cell32(f, b.i0 - kHalo, b.j0 + q, m);
+#pragma unroll
+  for (int k = 0; k < S::KV; ++k) {
+    const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
+    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
+      T hn, h = T(0.0), u = T(0.0), v;
+      if (i >= kHalo && i < m - kHalo) {
+        const int o = ov + r * m;
+        hn = hn_src[o];
+        if (blend) h = io.h[o];
+        v = io.v[o];
+        if (r >= kHalo && r < b.ni + kHalo) u = io.u[o];
+      } else {  // uncovered halo row: fetched point by point (the new h never has a stored halo)
+        hn = fetch_s(hn_src, g, f, i, b.j0 + q, 0);
+        if (blend) h = fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
+        fetch_v(io.u, io.v, g, f, i, b.j0 + q, io.stored_halo, u, v);
+      }
+      if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * h;  // fb_scheme, barotr_pure.py:52-54
+      hnv[k] = hn;
+      vvv[k] = v;
+      uvv[k] = u;
+    }
+  }
+  const int t6 = threadIdx.x;
+  const int sr = t6 / 6, sc = t6 - 6 * sr, scc = sc < 3 ? sc : b.nj + sc, sj = b.j0 - kHalo + scc;
+  const bool side_pt = t6 < 6 * b.ni && ec.col_staged(sj, m);
+  if (side_pt) {
+    T hn, h = T(0.0), v;
+    if (sj >= kHalo && sj < m - kHalo) {
+      const int o = cell32(f, b.i0 + sr, sj, m);
+      hn = hn_src[o];
+      if (blend) h = io.h[o];
+      us = io.u[o];
+    } else {
+      hn = fetch_s(hn_src, g, f, b.i0 + sr, sj, 0);
+      if (blend) h = fetch_s(io.h, g, f, b.i0 + sr, sj, io.stored_halo);
+      fetch_v(io.u, io.v, g, f, b.i0 + sr, sj, io.stored_halo, us, v);
+    }
+    if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * h;
+    hns = hn;
+  }
+#pragma unroll
+  for (int k = 0; k < S::KC; ++k) {
+    const int a = sl + k * S::NS;
+    if (q < b.nj && a < b.ni) {
+      upc[k] = io.up[ov + (a + kHalo) * m];
+      vpc[k] = io.vp[ov + (a + kHalo) * m];
+    }
+  }
+  if (P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr});
+#pragma unroll
+  for (int k = 0; k < S::KV; ++k) {
+    const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
+    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
+      L.s_hn[r * RJ + q + kHalo] = hnv[k];
+      L.s_v[r * TJ + q] = vvv[k];
+      if (r >= kHalo && r < b.ni + kHalo) L.s_u[(r - kHalo) * RJ + q + kHalo] = uvv[k];
+    }
+  }
+  if (side_pt) {
+    L.s_hn[(sr + kHalo) * RJ + scc] = hns;
+    L.s_u[sr * RJ + scc] = us;
+  }
   cp_async_wait_all();
   __syncthreads();
 
-  if (blend) {
+  // faces: upwind tangential component (remap.py:73-95) and kinetic energy (barotr_pure.py:91-92)
+  if (q < b.nj) {
 #pragma unroll
-    for (int it = 0; it < S::NIT; ++it) {
-      const int e = tid + it * kTileThreads;
-      if (e >= S::R) break;
-      const int r = e / RJ, c = e - r * RJ;
-      if (!region_needed(r, c, b.ni, b.nj)) continue;
-      s_hn[e] = (T(1.0) - io.beta) * s_hn[e] + io.beta * s_h[e];  // fb_scheme, barotr_pure.py:52-54
+    for (int k = 0; k < S::KX; ++k) {
+      const int a = sl + k * S::NS;
+      if (a <= b.ni) {
+        const int e = a * TJ + q;
+        const T* pt = L.s_v + a * TJ + q;
+        T p6[6];
+#pragma unroll
+        for (int z = 0; z < 6; ++z) p6[z] = pt[z * TJ];
+        const T bc = L.s_xc[e], vis = L.s_xc[S::FX + e];
+        const T vt = bc > T(0.0) ? rplus(p6, 1) : rminus(p6 + 1, 1);
+        L.s_ku[e] = T(0.5) * (vis * vis + vt * vt);
+        L.s_vx[e] = vt * L.s_cdy[e];
+      }
     }
   }
-  // faces: upwind tangential component (remap.py:73-95) and kinetic energy (barotr_pure.py:91-92)
-  for (int e = tid; e < S::FX + S::FY; e += kTileThreads) {
-    if (e < S::FX) {
-      const int a = e / TJ, q = e % TJ;
-      if (a > b.ni || q >= b.nj) continue;
-      const T* pt = s_v + a * RJ + (q + kHalo);
-      const T* c = s_xc + 3 * e;
-      const T vt = c[0] > T(0.0) ? rplus(pt, RJ) : rminus(pt + RJ, RJ);
-      s_ku[e] = T(0.5) * (c[1] * c[1] + vt * vt);
-      s_vx[e] = vt;
+#pragma unroll
+  for (int k = 0; k <= S::KC; ++k) {
+    int r, qq;
+    if (k < S::KC) {
+      r = sl + k * S::NS;
+      qq = q;
+      if (r >= b.ni || q > b.nj) continue;
     } else {
-      const int e2 = e - S::FX, a = e2 / (TJ + 1), q = e2 % (TJ + 1);
-      if (a >= b.ni || q > b.nj) continue;
-      const T* pt = s_u + (a + kHalo) * RJ + q;
-      const T* c = s_yc + 3 * e2;
-      const T ut = c[0] > T(0.0) ? rplus(pt, 1) : rminus(pt + 1, 1);
-      s_kv[e2] = T(0.5) * (c[1] * c[1] + ut * ut);
-      s_uy[e2] = ut;
+      r = threadIdx.x;
+      qq = TJ;
+      if (b.nj != TJ || r >= b.ni) continue;
     }
+    const int e = r * (TJ + 1) + qq;
+    const T* pt = L.s_u + r * RJ + qq;
+    T p6[6];
+#pragma unroll
+    for (int z = 0; z < 6; ++z) p6[z] = pt[z];
+    const T bc = L.s_yc[e], vis = L.s_yc[S::FY + e];
+    const T ut = bc > T(0.0) ? rplus(p6, 1) : rminus(p6 + 1, 1);
+    L.s_kv[e] = T(0.5) * (vis * vis + ut * ut);
+    L.s_uy[e] = ut * L.s_ddx[e];
   }
   __syncthreads();
 
-  for (int e = tid; e < S::C; e += kTileThreads) {
-    const int a = e / TJ, q = e % TJ;
-    if (a >= b.ni || q >= b.nj) continue;
-    const long o = cell(f, b.i0 + a, b.j0 + q, m);
-    const int xf0 = e, xf1 = e + TJ;
-    const int yf0 = a * (TJ + 1) + q, yf1 = yf0 + 1;
-    const int lc = (a + kHalo) * RJ + (q + kHalo);
-    const T* G = s_g + 4 * e;
-    const T u = s_u[lc], v = s_v[lc], sn = s_s[e];
-    const T uct = (G[0] * u + G[1] * v) * sn, vct = (G[2] * u + G[3] * v) * sn;  // remap.py:34-39
-    const T rdx = s_rdx[e], rdy = s_rdy[e];
-    // vorticity (agrid.py:31-41) and advection (barotr_pure.py:78-97)
-    const T vort = s_rda[e] * (s_uy[yf0] * s_ddx[yf0] + s_vx[xf1] * s_cdy[xf1] - s_uy[yf1] * s_ddx[yf1] -
-                               s_vx[xf0] * s_cdy[xf0]);
-    const T advx = vort * vct - (s_ku[xf1] - s_ku[xf0]) * rdx;
-    const T advy = -vort * uct - (s_kv[yf1] - s_kv[yf0]) * rdy;
-    // celerity viscosity (barotr_pure.py:63-75) from the cached face fluxes
-    const T visx = -(rdx * (s_xc[3 * xf1 + 2] - s_xc[3 * xf0 + 2]));
-    const T visy = -(rdy * (s_yc[3 * yf1 + 2] - s_yc[3 * yf0 + 2]));
-    // pressure gradient of the new h (agrid.py:55-69, barotr_pure.py:57-60)
-    const T* pbx = s_hn + (a * RJ + (q + kHalo));
-    const T* pby = s_hn + ((a + kHalo) * RJ + q);
-    const T pgu = T(-9.80) * (rdx * (mid6(pbx + RJ, RJ) - mid6(pbx, RJ)));
-    const T pgv = T(-9.80) * (rdy * (mid6(pby + 1, 1) - mid6(pby, 1)));
-    const T af = s_af[e];
-    // momentum update (barotr_pure.py:149-150)
-    io.u_out[o] = s_up[e] + (pgu + advx + af * vct + visx) * io.dt;
-    io.v_out[o] = s_vp[e] + (pgv + advy - af * uct + visy) * io.dt;
+  if (q < b.nj) {
+#pragma unroll
+    for (int k = 0; k < S::KC; ++k) {
+      const int a = sl + k * S::NS;
+      if (a >= b.ni) continue;
+      const int e = a * TJ + q;
+      const int xf0 = e, xf1 = e + TJ;
+      const int yf0 = a * (TJ + 1) + q, yf1 = yf0 + 1;
+      const T* G = L.s_g + 4 * e;
+      const T u = L.s_u[a * RJ + q + kHalo], v = L.s_v[(a + kHalo) * TJ + q], sn = L.s_sn[e];
+      const T uct = (G[0] * u + G[1] * v) * sn, vct = (G[2] * u + G[3] * v) * sn;  // remap.py:34-39
+      const T rdx = L.s_rdx[e], rdy = L.s_rdy[e];
+      // vorticity (agrid.py:31-41) and advection (barotr_pure.py:78-97)
+      const T vort = L.s_rda[e] * (L.s_uy[yf0] + L.s_vx[xf1] - L.s_uy[yf1] - L.s_vx[xf0]);
+      const T advx = vort * vct - (L.s_ku[xf1] - L.s_ku[xf0]) * rdx;
+      const T advy = -vort * uct - (L.s_kv[yf1] - L.s_kv[yf0]) * rdy;
+      // celerity viscosity (barotr_pure.py:63-75) from the cached face fluxes
+      const T visx = -(rdx * (L.s_xc[2 * S::FX + xf1] - L.s_xc[2 * S::FX + xf0]));
+      const T visy = -(rdy * (L.s_yc[2 * S::FY + yf1] - L.s_yc[2 * S::FY + yf0]));
+      // pressure gradient of the new h (agrid.py:55-69, barotr_pure.py:57-60)
+      const T* pbx = L.s_hn + (a * RJ + (q + kHalo));
+      const T* pby = L.s_hn + ((a + kHalo) * RJ + q);
+      T hx[7], hy[7];
+#pragma unroll
+      for (int z = 0; z < 7; ++z) {
+        hx[z] = pbx[z * RJ];
+        hy[z] = pby[z];
+      }
+      const T pgu = T(-9.80) * (rdx * (mid6(hx + 1, 1) - mid6(hx, 1)));
+      const T pgv = T(-9.80) * (rdy * (mid6(hy + 1, 1) - mid6(hy, 1)));
+      const T af = L.s_af[e];
+      // momentum update (barotr_pure.py:149-150)
+      const int o = ov + (a + kHalo) * m;
+      io.u_out[o] = upc[k] + (pgu + advx + af * vct + visx) * io.dt;
+      io.v_out[o] = vpc[k] + (pgv + advy - af * uct + visy) * io.dt;
+    }
   }
 }
 
@@ -917,6 +1127,7 @@ __device__ __forceinline__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, c
   wait_prior_grid();
   tile_uv_main<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
 }
+
 
 // ---------------------------------------------------------------------------
 // Grid-wide barrier of the persistent round kernel

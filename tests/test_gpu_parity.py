@@ -168,6 +168,26 @@ def test_tile_shapes_bitwise_identical(tile, grids):
         assert torch.equal(ref[k], got[k]), (tile, k)
 
 
+@pytest.mark.parametrize("n,tile", [(10, (8, 32)), (17, (8, 16)), (18, (16, 16)), (34, (4, 32))])
+def test_thin_last_tile_bitexact_against_oracle(n, tile, grids):
+    """N with a last tile 1 or 2 cells thin: the previous tile's stencil region
+    reaches the face halo without the tile touching that edge."""
+    g = grids(n)
+    consts = make_consts(g, 5000.0)
+    s = harmonic_state(g, 31)
+    m = n + 6
+    state = [s["h0"], s["h0"], s["ub"], s["vb"], s["ub"], s["vb"]] + [np.zeros((6, m, m))] * 17
+    dtb = cfl_dtb(g, 5000.0)
+    want = O.rk2_core(state, consts, 3, dtb)
+    p = BtPlan(consts, tile=tile)
+    got = p.round(*[dev(x) for x in state[:6]], nbb=3, dtb=dtb)
+    for k, name in ((0, "h0"), (2, "ub"), (3, "vb")):
+        assert_f64_close(got[name], want[k], f"C{n} {tile} {name}")
+    for k, name in enumerate(DIAG_NAMES):
+        assert_f64_close(got[name], want[6 + k], f"C{n} {tile} {name}")
+    p.close()
+
+
 def test_float32_precision_form_c48(grids):
     """FP32 state/consts vs the float64 reference run (config-1 case, 100 substeps)."""
     z = load_golden("rk2_c48_100.npz")
