@@ -21,7 +21,7 @@ from typing import List, Optional, Sequence, Tuple
 import torch
 
 from . import _native as N
-from .plan import DIAG_NAMES, BtPlan
+from .plan import cuda_device, DIAG_NAMES, BtPlan
 
 _MODES = {"persistent": N.BT_MODE_PERSISTENT, "stream": N.BT_MODE_STREAM}
 
@@ -86,7 +86,7 @@ class BtBatch:
             raise RuntimeError("licom4py_gpu_b200 needs a CUDA device (there is no CPU path)")
         if dtype not in (torch.float64, torch.float32):
             raise ValueError("dtype must be torch.float64 or torch.float32")
-        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.device = cuda_device(device)
         self.dtype = dtype
         self.max_members = int(max_members)
         h = ctypes.c_void_p()

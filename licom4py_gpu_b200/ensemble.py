@@ -23,7 +23,7 @@ from . import duogrid_gen
 from .batch import BtBatch, MemberState
 from .duogrid import make_consts
 from .fields import cfl_dtb, harmonic_state
-from .plan import BtPlan
+from .plan import cuda_device, BtPlan
 
 UV_PER_H = 0.3  # u, v RMS (m/s) per metre of h RMS: the 1 m / 0.3 m/s pairing of the seeded fields
 
@@ -59,7 +59,7 @@ class Geometry:
 
     def __init__(self, depth: float = 5000.0, device=None):
         self.depth = float(depth)
-        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.device = cuda_device(device)
         self._grids: Dict[int, dict] = {}
         self._plans: Dict[Tuple[int, torch.dtype], BtPlan] = {}
 

@@ -36,6 +36,14 @@ def _stream_handle(stream: Optional[torch.cuda.Stream]):
     return ctypes.c_void_p(s.cuda_stream)
 
 
+def cuda_device(device=None) -> torch.device:
+    """``device`` as an indexed CUDA device (None / "cuda" -> the current device)."""
+    d = torch.device(device) if device is not None else torch.device("cuda")
+    if d.type != "cuda":
+        raise ValueError(f"expected a CUDA device, got {d}")
+    return d if d.index is not None else torch.device("cuda", torch.cuda.current_device())
+
+
 def to_device(a, dtype: torch.dtype, device) -> torch.Tensor:
     """Contiguous CUDA tensor of ``dtype`` (numpy arrays are copied once)."""
     if isinstance(a, np.ndarray):
@@ -56,7 +64,7 @@ class BtPlan:
             raise ValueError(f"consts must hold the 17 CONST_SOURCES arrays, got {len(consts)}")
         if dtype not in (torch.float64, torch.float32):
             raise ValueError("dtype must be torch.float64 or torch.float32")
-        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.device = cuda_device(device)
         self.dtype = dtype
         with torch.cuda.device(self.device):
             tens = []
