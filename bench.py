@@ -68,6 +68,10 @@ def parse_args():
     p.add_argument("--case-only", action="store_true",
                    help="run one round of --nbb substeps (the profiling target) and exit, no timing")
     p.add_argument("--dtype", default="f64", choices=["f64", "f32"], help="dtype of --case-only")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the layered forms (precision at C384, batched ensemble, serving)")
+    p.add_argument("--serving-requests", type=int, default=150,
+                   help="requests of the Poisson serving stream in the bounded serving sample")
     return p.parse_args()
 
 
@@ -226,6 +230,186 @@ def run_reference(args, world, rank):
                              "sample": f"{sub} substeps per step x {args.steps} steps"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Layered forms: precision at C384, batched uneven ensemble, serving
+# ---------------------------------------------------------------------------
+def _rel(a, b):
+    """Relative L2 and max-norm error of a vs b over the interior cells (float64)."""
+    a = a[:, 3:-3, 3:-3].double()
+    b = b[:, 3:-3, 3:-3].double()
+    return float((a - b).norm() / b.norm()), float((a - b).abs().max() / b.abs().max())
+
+
+def form_precision(dev, depth, peak, seeds=8, nsub=2000):
+    """Float32 precision form vs float64 at C384: 2000 substeps from 8 seeded
+    states (h 1 m / u, v 0.3 m/s RMS); h/u/v errors, mass drift of both
+    precisions from compensated float64 sums, throughput of both."""
+    import torch
+    from licom4py_gpu_b200 import duogrid_gen
+    from licom4py_gpu_b200.autotune import choose_config
+    from licom4py_gpu_b200.duogrid import make_consts
+    from licom4py_gpu_b200.fields import cfl_dtb, harmonic_state
+    from licom4py_gpu_b200.momentum import conservation
+    from licom4py_gpu_b200.plan import BtPlan
+    n = 384
+    grid = duogrid_gen.generate(n)
+    consts = make_consts(grid, depth)
+    dtb = cfl_dtb(grid, depth)
+    rda = {}
+    c2l = {}
+    plans, times = {}, {torch.float64: 0.0, torch.float32: 0.0}
+    for dt in (torch.float64, torch.float32):
+        cfg = choose_config(n, dt, consts=consts, device=dev)
+        plans[dt] = BtPlan(consts, dtype=dt, device=dev, tile=tuple(cfg["tile"]), mode=cfg["mode"])
+        rda[dt] = torch.from_numpy(grid["rda"]).to(dev, dt)
+        c2l[dt] = torch.from_numpy(np.ascontiguousarray(grid["a_c2l"])).to(dev, dt)
+    err = {k: [0.0, 0.0] for k in ("h0", "ub", "vb")}
+    drift = {"f64": [], "f32": []}
+    da_abs = []
+    for seed in range(1, seeds + 1):
+        st = harmonic_state(grid, seed)
+        outs = {}
+        for dt in (torch.float64, torch.float32):
+            h, u, v = (torch.from_numpy(st[k]).to(dev, dt) for k in ("h0", "ub", "vb"))
+            p = plans[dt]
+            p.round(h, h, u, v, u, v, nbb=2, dtb=dtb, diag=False)  # warm the graph path
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            o = p.round(h, h, u, v, u, v, nbb=nsub, dtb=dtb, diag=False)
+            e1.record()
+            torch.cuda.synchronize()
+            times[dt] += e0.elapsed_time(e1)
+            m0 = conservation(h, u, v, rda[dt], c2l[dt], depth).cpu().numpy()
+            m1 = conservation(o["h0"], o["ub"], o["vb"], rda[dt], c2l[dt], depth).cpu().numpy()
+            outs[dt] = (o, m0, m1)
+        for k in err:
+            l2, li = _rel(outs[torch.float32][0][k], outs[torch.float64][0][k])
+            err[k][0] = max(err[k][0], l2)
+            err[k][1] = max(err[k][1], li)
+        hab = float((torch.from_numpy(np.abs(st["h0"][:, 3:-3, 3:-3]) / grid["rda"][:, 3:-3, 3:-3])).sum())
+        da_abs.append(hab)
+        for dt, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
+            _, m0, m1 = outs[dt]
+            drift[tag].append((m1[0] - m0[0]) / hab)
+    for p in plans.values():
+        p.close()
+    cu = 6 * n * n * nsub * seeds
+    v64, v32 = cu / (times[torch.float64] * 1e-3), cu / (times[torch.float32] * 1e-3)
+    return {"workload": f"C384, {nsub} RK2 substeps from {seeds} seeded states, float32 vs float64",
+            "reference": "float64 path of this library, bit-identical to the float64 oracle of the reference source",
+            "h_rel_l2": err["h0"][0], "h_rel_linf": err["h0"][1],
+            "u_rel_l2": err["ub"][0], "u_rel_linf": err["ub"][1],
+            "v_rel_l2": err["vb"][0], "v_rel_linf": err["vb"][1],
+            "mass_drift_f64": float(max(abs(x) for x in drift["f64"])),
+            "mass_drift_f32": float(max(abs(x) for x in drift["f32"])),
+            "mass_drift_error": float(max(abs(a - b) for a, b in zip(drift["f32"], drift["f64"]))),
+            "mass_drift_note": "mass sum(h da) change over the run / sum(|h0| da), compensated float64 sums",
+            "f64": {"value": v64, "unit": UNIT, "round_frac_of_hbm": v64 * B_ALG_WORDS * 8 / 1e9 / peak},
+            "f32": {"value": v32, "unit": UNIT, "round_frac_of_hbm": v32 * B_ALG_WORDS * 4 / 1e9 / peak}}
+
+
+def form_ensemble(dev, depth):
+    """Batched uneven ensemble (32 x C48, 24 x C96, 8 x C192; amplitudes
+    U[0.2, 2] m, substeps U{200..2000}), float32, autotuned batch schedule:
+    one persistent launch runs every member to its end.  Against the same
+    members run one integration per launch through the drop-in path."""
+    import torch
+    from licom4py_gpu_b200 import autotune
+    from licom4py_gpu_b200.batch import BtBatch
+    from licom4py_gpu_b200.duogrid import make_consts
+    from licom4py_gpu_b200.ensemble import Ensemble, Geometry, PlainRunner, uneven_mix
+    specs = uneven_mix()
+    geo = Geometry(depth, device=dev)
+    ens = Ensemble(specs, torch.float32, geometry=geo)
+    cfg = autotune.choose_batch_config(ens)
+    b = BtBatch(torch.float32, max_members=len(specs), device=dev, mode=cfg["mode"], tile=tuple(cfg["tile"]))
+    b.set_max_ctas(cfg.get("max_ctas", 0))
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts), r
+
+    work = ens.cell_updates()
+    ens.run_batched(b)
+    ms_b, mem32 = timed(lambda: ens.run_batched(b), 3)
+    b.check_device_error()
+    singles = {n: autotune.choose_config(n, torch.float32, consts=make_consts(geo.grid(n), depth), device=dev)
+               for n in sorted({s.n for s in specs})}
+    pr = PlainRunner(ens, singles)
+    pr.run()
+    ms_p, _ = timed(pr.run, 2)
+    pr.close()
+    # accuracy: every member against its float64 integration
+    ens64 = Ensemble(specs, torch.float64, geometry=geo)
+    b64 = BtBatch(torch.float64, max_members=len(specs), device=dev)
+    mem64 = ens64.run_batched(b64)
+    torch.cuda.synchronize()
+    l2 = max(_rel(a.state[0], c.state[0])[0] for a, c in zip(mem32, mem64))
+    li = max(_rel(a.state[0], c.state[0])[1] for a, c in zip(mem32, mem64))
+    b.close()
+    b64.close()
+    geo.close()
+    vb, vp = work / (ms_b * 1e-3), work / (ms_p * 1e-3)
+    return {"workload": "64 members (32 x C48, 24 x C96, 8 x C192), amplitude U[0.2, 2] m, substeps U{200..2000}, "
+                        "RK2, float32; one persistent launch for the whole run, members retire early",
+            "cell_updates": work, "batched": {"value": vb, "unit": UNIT, "ms": ms_b,
+                                              "schedule": {k: cfg[k] for k in ("mode", "tile", "max_ctas", "source")
+                                                           if k in cfg}},
+            "plain_one_per_launch": {"value": vp, "unit": UNIT, "ms": ms_p,
+                                     "configs": {str(k): [v["mode"], v["tile"]] for k, v in singles.items()}},
+            "speedup": vb / vp, "h_rel_l2_max_vs_f64": l2, "h_rel_linf_max_vs_f64": li}
+
+
+def form_serving(dev, depth, count):
+    """Serving sample: the first ``count`` requests of the Poisson stream
+    (200 req/s; C48 0.4, C96 0.35, C192 0.2, C384 0.05; substeps log-uniform
+    in [100, 5000]), float32, served with continuous batching (rounds of 200
+    substeps, admission by an HBM budget of half the free memory) and by the
+    FIFO one-at-a-time plain path, both in real time on the same GPU."""
+    import torch
+    from licom4py_gpu_b200.ensemble import Geometry
+    from licom4py_gpu_b200.serving import BarotropicServer, Request, poisson_mix, run_fifo
+    geo = Geometry(depth, device=dev)
+    for n in (48, 96, 192, 384):
+        geo.plan(n, torch.float32)
+        geo.dtb(n)
+    reqs = poisson_mix(count=count, rate=200.0, seed=0)
+    srv = BarotropicServer(geo, dtype=torch.float32, round_substeps=200)
+    for n in (48, 96, 192, 384):
+        srv.basis._get(n)
+    torch.cuda.synchronize()
+    st = srv.run(reqs, realtime=True)
+    srv.close()
+    reqs_f = poisson_mix(count=count, rate=200.0, seed=0)
+    sf = run_fifo(geo, reqs_f, dtype=torch.float32, realtime=True)
+    same = max(float(np.abs(a.result["h0"] - b.result["h0"]).max() / np.abs(b.result["h0"]).max())
+               for a, b in zip(reqs, reqs_f))
+    # float64 check of the smallest requests (each alone, float64)
+    small = sorted(reqs, key=lambda r: r.cell_updates)[:8]
+    ref = [Request(rid=r.rid, n=r.n, nsub=r.nsub, seed=r.seed) for r in small]
+    run_fifo(geo, ref, dtype=torch.float64, realtime=False)
+    err64 = max(float(np.linalg.norm(a.result["h0"][:, 3:-3, 3:-3] - b.result["h0"][:, 3:-3, 3:-3]) /
+                      np.linalg.norm(b.result["h0"][:, 3:-3, 3:-3])) for a, b in zip(small, ref))
+    geo.close()
+    keep = ("p50_s", "p99_s", "mean_s", "max_s", "requests", "wall_s", "cell_updates_per_s")
+    return {"workload": f"first {count} requests of the 10k-request Poisson stream at 200 req/s "
+                        f"(arrival span {reqs[-1].arrival:.2f} s), float32, RK2",
+            "continuous_batching": {k: st[k] for k in keep + ("rounds",)},
+            "fifo_plain": {k: sf[k] for k in keep},
+            "throughput_ratio": st["cell_updates_per_s"] / sf["cell_updates_per_s"],
+            "same_result_alone_vs_mix_h_rel_max": same,
+            "h_rel_l2_vs_f64_smallest8": err64}
 
 
 # ---------------------------------------------------------------------------
@@ -423,6 +607,11 @@ def run_ours(args, world, rank, local):
                         "round_frac_of_hbm": cu * B_ALG_WORDS * esz / 1e9 / peak,
                         "kernel": kernel_roofline(384, dt_, t384, 100, c384, s384, d384)}
         extras["c384"] = big
+
+    if not args.no_forms and world == 1:
+        extras["precision_c384"] = form_precision(dev, args.depth, peak)
+        extras["ensemble"] = form_ensemble(dev, args.depth)
+        extras["serving"] = form_serving(dev, args.depth, args.serving_requests)
 
     cpu = None
     if rank == 0 and world == 1:
