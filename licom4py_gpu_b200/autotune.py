@@ -15,7 +15,7 @@ from typing import Dict, Optional, Sequence
 
 import torch
 
-TILES = ((4, 32), (8, 32), (16, 32), (8, 16), (16, 16))
+TILES = ((7, 32), (8, 32), (15, 32), (16, 32), (8, 16), (16, 16))
 MODES = ("persistent", "graph")
 
 

@@ -285,14 +285,12 @@ cudaError_t launch_batch_phase_tile(const BatchArgs<T>& a, int step, int st, int
 template <typename T, bool UV>
 cudaError_t batch_phase_dispatch(const BatchArgs<T>& a, TileCfg c, int step, int st, int act, int ntiles,
                                  cudaStream_t s) {
-  if (c.tj == 32) {
-    if (c.ti == 4) return launch_batch_phase_tile<T, 4, 32, UV>(a, step, st, act, ntiles, s);
-    if (c.ti == 8) return launch_batch_phase_tile<T, 8, 32, UV>(a, step, st, act, ntiles, s);
-    if (c.ti == 16) return launch_batch_phase_tile<T, 16, 32, UV>(a, step, st, act, ntiles, s);
-  } else if (c.tj == 16) {
-    if (c.ti == 8) return launch_batch_phase_tile<T, 8, 16, UV>(a, step, st, act, ntiles, s);
-    if (c.ti == 16) return launch_batch_phase_tile<T, 16, 16, UV>(a, step, st, act, ntiles, s);
-  }
+  if (c.ti == 7 && c.tj == 32) return launch_batch_phase_tile<T, 7, 32, UV>(a, step, st, act, ntiles, s);
+  if (c.ti == 8 && c.tj == 32) return launch_batch_phase_tile<T, 8, 32, UV>(a, step, st, act, ntiles, s);
+  if (c.ti == 15 && c.tj == 32) return launch_batch_phase_tile<T, 15, 32, UV>(a, step, st, act, ntiles, s);
+  if (c.ti == 16 && c.tj == 32) return launch_batch_phase_tile<T, 16, 32, UV>(a, step, st, act, ntiles, s);
+  if (c.ti == 8 && c.tj == 16) return launch_batch_phase_tile<T, 8, 16, UV>(a, step, st, act, ntiles, s);
+  if (c.ti == 16 && c.tj == 16) return launch_batch_phase_tile<T, 16, 16, UV>(a, step, st, act, ntiles, s);
   return cudaErrorInvalidValue;
 }
 
@@ -315,8 +313,9 @@ cudaError_t launch_small(void (*kern)(BatchArgs<T>), const BatchArgs<T>& a, int 
 template <typename T>
 cudaError_t prime_batch() {
   cudaError_t e;
-  if ((e = prime_batch_tile<T, 4, 32>()) != cudaSuccess) return e;
+  if ((e = prime_batch_tile<T, 7, 32>()) != cudaSuccess) return e;
   if ((e = prime_batch_tile<T, 8, 32>()) != cudaSuccess) return e;
+  if ((e = prime_batch_tile<T, 15, 32>()) != cudaSuccess) return e;
   if ((e = prime_batch_tile<T, 16, 32>()) != cudaSuccess) return e;
   if ((e = prime_batch_tile<T, 8, 16>()) != cudaSuccess) return e;
   return prime_batch_tile<T, 16, 16>();
@@ -325,14 +324,12 @@ cudaError_t prime_batch() {
 template <typename T>
 cudaError_t launch_batch_round(const BatchArgs<T>& a, TileCfg c, int max_tiles, int max_ctas, cudaStream_t s,
                                int* grid_out) {
-  if (c.tj == 32) {
-    if (c.ti == 4) return launch_batch_round_tile<T, 4, 32>(a, max_tiles, max_ctas, s, grid_out);
-    if (c.ti == 8) return launch_batch_round_tile<T, 8, 32>(a, max_tiles, max_ctas, s, grid_out);
-    if (c.ti == 16) return launch_batch_round_tile<T, 16, 32>(a, max_tiles, max_ctas, s, grid_out);
-  } else if (c.tj == 16) {
-    if (c.ti == 8) return launch_batch_round_tile<T, 8, 16>(a, max_tiles, max_ctas, s, grid_out);
-    if (c.ti == 16) return launch_batch_round_tile<T, 16, 16>(a, max_tiles, max_ctas, s, grid_out);
-  }
+  if (c.ti == 7 && c.tj == 32) return launch_batch_round_tile<T, 7, 32>(a, max_tiles, max_ctas, s, grid_out);
+  if (c.ti == 8 && c.tj == 32) return launch_batch_round_tile<T, 8, 32>(a, max_tiles, max_ctas, s, grid_out);
+  if (c.ti == 15 && c.tj == 32) return launch_batch_round_tile<T, 15, 32>(a, max_tiles, max_ctas, s, grid_out);
+  if (c.ti == 16 && c.tj == 32) return launch_batch_round_tile<T, 16, 32>(a, max_tiles, max_ctas, s, grid_out);
+  if (c.ti == 8 && c.tj == 16) return launch_batch_round_tile<T, 8, 16>(a, max_tiles, max_ctas, s, grid_out);
+  if (c.ti == 16 && c.tj == 16) return launch_batch_round_tile<T, 16, 16>(a, max_tiles, max_ctas, s, grid_out);
   return cudaErrorInvalidValue;
 }
 

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kThreads) k_diag(Geo<T> g, const T* h, const T
 
 #ifdef BT_DEFINE_COMMON
 bool tile_cfg_supported(TileCfg c) {
-  return (c.tj == 32 && (c.ti == 4 || c.ti == 8 || c.ti == 16)) ||
+  return (c.tj == 32 && (c.ti == 7 || c.ti == 8 || c.ti == 15 || c.ti == 16)) ||
          (c.tj == 16 && (c.ti == 8 || c.ti == 16));
 }
 
@@ -200,14 +200,12 @@ cudaError_t launch_tile(const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
 
 template <typename T, bool UV>
 cudaError_t dispatch(const Geo<T>& g, const StageIO<T>& io, TileCfg c, cudaStream_t s) {
-  if (c.tj == 32) {
-    if (c.ti == 4) return launch_tile<T, 4, 32, UV>(g, io, s);
-    if (c.ti == 8) return launch_tile<T, 8, 32, UV>(g, io, s);
-    if (c.ti == 16) return launch_tile<T, 16, 32, UV>(g, io, s);
-  } else if (c.tj == 16) {
-    if (c.ti == 8) return launch_tile<T, 8, 16, UV>(g, io, s);
-    if (c.ti == 16) return launch_tile<T, 16, 16, UV>(g, io, s);
-  }
+  if (c.ti == 7 && c.tj == 32) return launch_tile<T, 7, 32, UV>(g, io, s);
+  if (c.ti == 8 && c.tj == 32) return launch_tile<T, 8, 32, UV>(g, io, s);
+  if (c.ti == 15 && c.tj == 32) return launch_tile<T, 15, 32, UV>(g, io, s);
+  if (c.ti == 16 && c.tj == 32) return launch_tile<T, 16, 32, UV>(g, io, s);
+  if (c.ti == 8 && c.tj == 16) return launch_tile<T, 8, 16, UV>(g, io, s);
+  if (c.ti == 16 && c.tj == 16) return launch_tile<T, 16, 16, UV>(g, io, s);
   return cudaErrorInvalidValue;
 }
 
@@ -215,22 +213,21 @@ cudaError_t dispatch(const Geo<T>& g, const StageIO<T>& io, TileCfg c, cudaStrea
 
 template <typename T>
 cudaError_t launch_round(const RoundArgs<T>& a, TileCfg c, int max_ctas, cudaStream_t s, int* grid_out) {
-  if (c.tj == 32) {
-    if (c.ti == 4) return launch_round_tile<T, 4, 32>(a, max_ctas, s, grid_out);
-    if (c.ti == 8) return launch_round_tile<T, 8, 32>(a, max_ctas, s, grid_out);
-    if (c.ti == 16) return launch_round_tile<T, 16, 32>(a, max_ctas, s, grid_out);
-  } else if (c.tj == 16) {
-    if (c.ti == 8) return launch_round_tile<T, 8, 16>(a, max_ctas, s, grid_out);
-    if (c.ti == 16) return launch_round_tile<T, 16, 16>(a, max_ctas, s, grid_out);
-  }
+  if (c.ti == 7 && c.tj == 32) return launch_round_tile<T, 7, 32>(a, max_ctas, s, grid_out);
+  if (c.ti == 8 && c.tj == 32) return launch_round_tile<T, 8, 32>(a, max_ctas, s, grid_out);
+  if (c.ti == 15 && c.tj == 32) return launch_round_tile<T, 15, 32>(a, max_ctas, s, grid_out);
+  if (c.ti == 16 && c.tj == 32) return launch_round_tile<T, 16, 32>(a, max_ctas, s, grid_out);
+  if (c.ti == 8 && c.tj == 16) return launch_round_tile<T, 8, 16>(a, max_ctas, s, grid_out);
+  if (c.ti == 16 && c.tj == 16) return launch_round_tile<T, 16, 16>(a, max_ctas, s, grid_out);
   return cudaErrorInvalidValue;
 }
 
 template <typename T>
 cudaError_t prime_kernels() {
   cudaError_t e;
-  if ((e = prime_tile<T, 4, 32>()) != cudaSuccess) return e;
+  if ((e = prime_tile<T, 7, 32>()) != cudaSuccess) return e;
   if ((e = prime_tile<T, 8, 32>()) != cudaSuccess) return e;
+  if ((e = prime_tile<T, 15, 32>()) != cudaSuccess) return e;
   if ((e = prime_tile<T, 16, 32>()) != cudaSuccess) return e;
   if ((e = prime_tile<T, 8, 16>()) != cudaSuccess) return e;
   return prime_tile<T, 16, 16>();

@@ -211,6 +211,7 @@ constexpr int up4(int x) { return (x + 3) & ~3; }  // shared-memory offsets in w
 template <int TI, int TJ>
 struct TileShape {
   static_assert(TJ == 16 || TJ == 32, "tile columns must be 16 or 32");
+  static_assert(TI <= 32, "the east y-face column is one lane per tile row");
   static constexpr int RI = TI + 6, RJ = TJ + 6;
   static constexpr int NS = kTileThreads / TJ;      // row slots
   static constexpr int VB = RI * TJ;                // vertical-bar points (r * TJ + q)
@@ -263,6 +264,17 @@ __device__ __forceinline__ TileBox tile_box(const Tiling& t, int n, int tile) {
 
 // 32-bit offset of cell (i, j) of face f (fields of up to 2^31 elements).
 __device__ __forceinline__ int cell32(int f, int i, int j, int m) { return (f * m + i) * m + j; }
+
+// Row handled by this thread in the tile's east y-face column (faces at column
+// TJ of full-width tiles): lane r of the last warp.  With TI = 8k - 1 rows the
+// x-face rows (TI + 1) fill every warp evenly and the last warp has one tile
+// row fewer, so the extra column evens out the face work across the warps.
+__device__ __forceinline__ int east_row() { return (int)threadIdx.x - (kTileThreads - 32); }
+
+// Face-cache entries: x face (f, i', j') at (f (n + 1) + i') n + j', y face at
+// (f n + i') (n + 1) + j'; the three cached values sit in planes 6 (n + 1) n apart.
+__device__ __forceinline__ int xface_idx(int f, int ip, int jp, int n) { return (f * (n + 1) + ip) * n + jp; }
+__device__ __forceinline__ int yface_idx(int f, int ip, int jp, int n) { return (f * n + ip) * (n + 1) + jp; }
 
 // ---- asynchronous global -> shared copies ---------------------------------
 template <int BYTES>
@@ -666,8 +678,8 @@ __device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io
       }
     }
   }
-  if (b.nj == TJ && threadIdx.x < b.ni) {  // the last y-face column of full-width tiles
-    const int r = threadIdx.x, o = cell32(b.f, b.i0 + r, b.j0 + TJ, m);
+  if (b.nj == TJ && east_row() >= 0 && east_row() < b.ni) {  // the last y-face column of full-width tiles
+    const int r = east_row(), o = cell32(b.f, b.i0 + r, b.j0 + TJ, m);
     cp_async_t(L.s_dzy + r * (TJ + 1) + TJ, g.dzph_y + o);
     cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + o);
   }
@@ -683,7 +695,7 @@ __device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io
 template <typename T>
 __device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, const T* pu, int su, int side,
                                     int slot, T dz, const T* s_np, const T* s_nh, const T* s_ndz, T* fc,
-                                    long pstride) {
+                                    int pstride) {
   T hh[6], uu[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
@@ -789,7 +801,7 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
   __syncthreads();
 
   // faces; their fluxes (times c_dy / d_dx) alias the metric block, no longer read
-  const long PF = 6L * (n + 1) * n;  // plane size of both face caches
+  const int PF = 6 * (n + 1) * n;  // plane size of both face caches
   if (q < b.nj) {
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
@@ -798,7 +810,7 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
         const int side = (a == 0 && b.i0 == kHalo) ? kS : ((a == b.ni && b.i0 + b.ni == m - kHalo) ? kN : -1);
         const int e = a * TJ + q;
         T* fc = (a < b.ni || side == kN)
-                    ? io.fx + (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q))
+                    ? io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n)
                     : nullptr;
         const T fl = face_h<T>(io, L.s_h + a * RJ + q + kHalo, RJ, L.s_uc + a * TJ + q, TJ, side,
                                (side == kS ? 0 : 1) * S::EW + q, L.s_dzx[e], L.s_np, L.s_nh, L.s_ndz, fc, PF);
@@ -806,7 +818,7 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
       }
     }
   }
-  // y faces: (r, qq) with qq = q, plus qq = TJ for full-width tiles (threads < ni)
+  // y faces: (r, qq) with qq = q, plus qq = TJ for full-width tiles (lanes of the last warp)
 #pragma unroll
   for (int k = 0; k <= S::KC; ++k) {
     int r, qq;
@@ -815,14 +827,14 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
       qq = q;
       if (r >= b.ni || q > b.nj) continue;
     } else {
-      r = threadIdx.x;
+      r = east_row();
       qq = TJ;
-      if (b.nj != TJ || r >= b.ni) continue;
+      if (b.nj != TJ || r < 0 || r >= b.ni) continue;
     }
     const int side = (qq == 0 && b.j0 == kHalo) ? kW : ((qq == b.nj && b.j0 + b.nj == m - kHalo) ? kE : -1);
     const int e = r * (TJ + 1) + qq;
     T* fc = (qq < b.nj || side == kE)
-                ? io.fy + (((long)f * n + (b.i0 - kHalo + r)) * (n + 1) + (b.j0 - kHalo + qq))
+                ? io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n)
                 : nullptr;
     const T fl = face_h<T>(io, L.s_h + (r + kHalo) * RJ + qq, 1, L.s_vc + r * RJ + qq, 1, side,
                            (side == kW ? 2 : 3) * S::EW + r, L.s_dzy[e], L.s_np, L.s_nh, L.s_ndz, fc, PF);
@@ -906,8 +918,8 @@ __device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& i
       if (r < b.ni) cp_async_t(L.s_ddx + r * (TJ + 1) + q, g.d_dx + o0 + r * m);
     }
   }
-  if (b.nj == TJ && threadIdx.x < b.ni) {
-    const int r = threadIdx.x;
+  if (b.nj == TJ && east_row() >= 0 && east_row() < b.ni) {
+    const int r = east_row();
     cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + cell32(b.f, b.i0 + r, b.j0 + TJ, m));
   }
   P = edge_count(b, m, cnt);
@@ -924,7 +936,7 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
   const LayoutUV<T, TI, TJ> L(sm);
   const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
   const T* hn_src = (const T*)io.h_out;
-  const long PF = 6L * (n + 1) * n;
+  const int PF = 6 * (n + 1) * n;
 
   // face caches of this stage (written by phase H) -> shared memory
   if (q < b.nj) {
@@ -932,7 +944,7 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
     for (int k = 0; k < S::KX; ++k) {
       const int a = sl + k * S::NS;
       if (a <= b.ni) {
-        const T* src = io.fx + (((long)f * (n + 1) + (b.i0 - kHalo + a)) * n + (b.j0 - kHalo + q));
+        const T* src = io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n);
         const int e = a * TJ + q;
         cp_async_t(L.s_xc + e, src);
         cp_async_t(L.s_xc + S::FX + e, src + PF);
@@ -948,11 +960,11 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
       qq = q;
       if (r >= b.ni || q > b.nj) continue;
     } else {
-      r = threadIdx.x;
+      r = east_row();
       qq = TJ;
-      if (b.nj != TJ || r >= b.ni) continue;
+      if (b.nj != TJ || r < 0 || r >= b.ni) continue;
     }
-    const T* src = io.fy + (((long)f * n + (b.i0 - kHalo + r)) * (n + 1) + (b.j0 - kHalo + qq));
+    const T* src = io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n);
     const int e = r * (TJ + 1) + qq;
     cp_async_t(L.s_yc + e, src);
     cp_async_t(L.s_yc + S::FY + e, src + PF);
@@ -1055,9 +1067,9 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
       qq = q;
       if (r >= b.ni || q > b.nj) continue;
     } else {
-      r = threadIdx.x;
+      r = east_row();
       qq = TJ;
-      if (b.nj != TJ || r >= b.ni) continue;
+      if (b.nj != TJ || r < 0 || r >= b.ni) continue;
     }
     const int e = r * (TJ + 1) + qq;
     const T* pt = L.s_u + r * RJ + qq;
