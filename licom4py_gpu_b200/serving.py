@@ -22,6 +22,7 @@ path used for comparison.
 
 from __future__ import annotations
 
+import heapq
 import math
 import time
 from collections import deque
@@ -78,18 +79,25 @@ class Scheduler:
     """Admission and round planning, host only.
 
     ``member_bytes(n)`` gives the device bytes one request of resolution n
-    holds while admitted.  Requests are admitted strictly in arrival order
-    (no overtaking, so a large request is not starved) while the budget and
-    ``max_members`` allow; a request larger than the whole budget is rejected.
+    holds while admitted.  Waiting requests are admitted while the budget and
+    ``max_members`` allow, in the order ``order`` gives: "fifo" = arrival
+    order with no overtaking (a large request is never starved), "shortest" =
+    least work (cell-updates) first, arrival order among equals (lower median
+    latency when the server is overloaded, at the cost of the largest
+    requests).  A request larger than the whole budget is rejected.
     """
 
     def __init__(self, budget: int, member_bytes: Callable[[int], int], max_members: int = 1024,
-                 round_substeps: int = 200):
+                 round_substeps: int = 200, order: str = "fifo"):
+        if order not in ("fifo", "shortest"):
+            raise ValueError("order must be 'fifo' or 'shortest'")
         self.budget = int(budget)
         self.member_bytes = member_bytes
         self.max_members = int(max_members)
         self.round_substeps = int(round_substeps)
+        self.order = order
         self.waiting: Deque[Request] = deque()
+        self._heap: List[Tuple[int, float, int, Request]] = []
         self.active: Dict[int, Tuple[Request, int]] = {}  # rid -> (request, substeps left)
         self.used = 0
         self.peak = 0  # largest budget use seen
@@ -98,17 +106,36 @@ class Scheduler:
     def arrive(self, req: Request) -> None:
         if self.member_bytes(req.n) > self.budget:
             self.rejected.append(req)
-        else:
+        elif self.order == "fifo":
             self.waiting.append(req)
+        else:
+            heapq.heappush(self._heap, (req.cell_updates, req.arrival, req.rid, req))
+
+    def _next(self) -> Optional[Request]:
+        if self.order == "fifo":
+            return self.waiting[0] if self.waiting else None
+        return self._heap[0][3] if self._heap else None
+
+    def _pop(self) -> None:
+        if self.order == "fifo":
+            self.waiting.popleft()
+        else:
+            heapq.heappop(self._heap)
+
+    @property
+    def queued(self) -> int:
+        return len(self.waiting) + len(self._heap)
 
     def admit(self) -> List[Request]:
         out = []
-        while self.waiting and len(self.active) < self.max_members:
-            req = self.waiting[0]
+        while len(self.active) < self.max_members:
+            req = self._next()
+            if req is None:
+                break
             need = self.member_bytes(req.n)
             if self.used + need > self.budget:
                 break
-            self.waiting.popleft()
+            self._pop()
             self.used += need
             self.peak = max(self.peak, self.used)
             self.active[req.rid] = (req, req.nsub)
@@ -135,7 +162,7 @@ class Scheduler:
 
     @property
     def idle(self) -> bool:
-        return not self.waiting and not self.active
+        return self.queued == 0 and not self.active
 
 
 def latency_stats(reqs: Sequence[Request]) -> Dict[str, float]:
@@ -218,8 +245,9 @@ class BarotropicServer:
     """Continuous-batching executor of :class:`Scheduler` on one GPU."""
 
     def __init__(self, geometry, dtype=None, rk: int = 2, round_substeps: int = 200,
-                 hbm_budget: Optional[int] = None, max_members: int = 1024, mode: str = "persistent",
-                 tile: Tuple[int, int] = (8, 32), max_ctas: int = 0, keep_results: bool = True):
+                 hbm_budget: Optional[int] = None, max_members: int = 1024, mode: str = "stream",
+                 tile: Tuple[int, int] = (16, 32), max_ctas: int = 0, keep_results: bool = True,
+                 order: str = "fifo"):
         import torch
         from .batch import BtBatch, member_bytes
         self.torch = torch
@@ -236,7 +264,7 @@ class BarotropicServer:
             if n not in self._mbytes:
                 self._mbytes[n] = member_bytes(self.geo.plan(n, self.dtype), self.rk)
             return self._mbytes[n]
-        self.sched = Scheduler(hbm_budget, mb, max_members, round_substeps)
+        self.sched = Scheduler(hbm_budget, mb, max_members, round_substeps, order)
         self.batch = BtBatch(self.dtype, max_members=max_members, device=self.device, mode=mode, tile=tile)
         self.batch.set_max_ctas(max_ctas)
         self.basis = HarmonicBasis(geometry, self.device)

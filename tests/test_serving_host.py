@@ -62,3 +62,21 @@ def test_latency_stats():
         r.t_done = (k + 1) / 100.0
     st = latency_stats(reqs)
     assert abs(st["p50_s"] - 0.505) < 1e-9 and abs(st["p99_s"] - 0.9901) < 1e-9
+
+
+def test_scheduler_shortest_first_order():
+    s = Scheduler(budget=100, member_bytes=lambda n: 10, max_members=2, round_substeps=10, order="shortest")
+    work = [(48, 900), (12, 50), (24, 30), (12, 10)]
+    for k, (n, ns) in enumerate(work):
+        s.arrive(Request(rid=k, n=n, nsub=ns, seed=k, arrival=0.1 * k))
+    assert s.queued == 4
+    assert [r.rid for r in s.admit()] == [3, 1]      # 6*12^2*10, then 6*12^2*50 cell-updates
+    s.finish_round(s.plan_round())                    # rid 3 done
+    assert [r.rid for r in s.admit()] == [2]
+    assert s.queued == 1
+
+
+def test_scheduler_rejects_unknown_order():
+    import pytest
+    with pytest.raises(ValueError):
+        Scheduler(budget=1, member_bytes=lambda n: 1, order="lifo")
