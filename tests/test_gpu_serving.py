@@ -28,11 +28,12 @@ def geo():
     g.close()
 
 
-@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-def test_results_same_alone_and_in_the_mix(dtype, geo):
+@pytest.mark.parametrize("dtype,order", [(torch.float32, "fifo"), (torch.float64, "fifo"),
+                                         (torch.float32, "shortest")])
+def test_results_same_alone_and_in_the_mix(dtype, order, geo):
     reqs = [Request(rid=k, n=n, nsub=ns, seed=100 + 3 * k, arrival=0.0) for k, (n, ns) in enumerate(MIX)]
     budget = 3 * member_bytes(geo.plan(24, dtype), 2)
-    srv = BarotropicServer(geo, dtype=dtype, round_substeps=8, hbm_budget=budget, max_members=8)
+    srv = BarotropicServer(geo, dtype=dtype, round_substeps=8, hbm_budget=budget, max_members=8, order=order)
     stats = srv.run(reqs, realtime=False)
     srv.close()
     assert stats["requests"] == len(MIX) and stats["rejected"] == 0
