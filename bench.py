@@ -95,32 +95,18 @@ def run_case(args):
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    return world, rank, local
+    from licom4py_gpu_b200 import replicas
+    return replicas.setup("nccl")
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from licom4py_gpu_b200 import replicas
+    replicas.barrier()
 
 
 def max_over_ranks(x, world):
-    if world <= 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from licom4py_gpu_b200 import replicas
+    return replicas.max_over_ranks(x)
 
 
 def build_problem(n, depth, seed):
@@ -663,9 +649,8 @@ def main():
         else:
             run_ours(args, world, rank, local)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        from licom4py_gpu_b200 import replicas
+        replicas.teardown()
 
 
 if __name__ == "__main__":
