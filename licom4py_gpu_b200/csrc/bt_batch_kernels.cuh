@@ -32,6 +32,24 @@ __device__ __forceinline__ int member_of(const int* off, int count, int item) {
   return lo;
 }
 
+// The same search by one warp: each round the 32 lanes test 32 evenly spaced
+// offsets of the remaining range at once, so a list of up to 32 members takes
+// one load round trip and up to 1024 two.  Every lane returns the result.
+__device__ __forceinline__ int member_of_warp(const int* off, int count, int item) {
+  const int lane = threadIdx.x & 31;
+  int lo = 0, hi = count;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const int step = (hi - lo + 31) >> 5;
+    const int idx = lo + lane * step;
+    const bool le = idx < hi && __ldg(off + idx) <= item;
+    const unsigned m = __ballot_sync(0xffffffffu, le);  // lane 0 always set: off[lo] <= item
+    const int last = 31 - __clz(m);
+    lo += last * step;
+    hi = min(hi, lo + step);
+  }
+  return lo;
+}
+
 // Stage pointers of member k at (substep, stage); the schedule of
 // barotr.py:41-87 as in the single-member round.
 template <typename T>
@@ -67,30 +85,36 @@ __device__ StageIO<T> member_stage(const MemberDesc<T>& d, int rk, int step, int
   return io;
 }
 
-// Shared-memory copies of the current tile's member geometry and stage
-// pointers; the tile code reads them like kernel parameters.
+// Shared-memory copies of the current tile's member record, geometry and
+// stage pointers; the tile code reads them like kernel parameters.
 template <typename T>
 struct TileCtx {
+  MemberDesc<T> d;
   Geo<T> g;
   StageIO<T> io;
-  int k;  // member whose geometry is in g (-1: none)
+  int k;  // member whose record and geometry are loaded (-1: none)
 };
 
 // Point ctx at member k, stage (step, st).  Called by every thread between
-// barriers: warp 0 copies the geometry when the member changes, thread 0
-// writes the stage pointers.
+// barriers; warp 0 alone does the work: when the member changes it copies the
+// member record and then its geometry with coalesced word loads (two round
+// trips), and lane 0 derives the stage pointers from the copy.
 template <typename T>
 __device__ __forceinline__ void ctx_load(TileCtx<T>& ctx, const BatchArgs<T>& a, int k, int step, int st) {
   __syncthreads();  // the previous tile is done with ctx
-  if (ctx.k != k) {
-    const int gi = a.mem[k].geo;
-    if (threadIdx.x < 32) {
-      const int* src = reinterpret_cast<const int*>(a.geos + gi);
-      int* dst = reinterpret_cast<int*>(&ctx.g);
-      for (int w = threadIdx.x; w < (int)(sizeof(Geo<T>) / sizeof(int)); w += 32) dst[w] = __ldg(src + w);
+  if (threadIdx.x < 32) {
+    if (ctx.k != k) {
+      const int* src = reinterpret_cast<const int*>(a.mem + k);
+      int* dst = reinterpret_cast<int*>(&ctx.d);
+      for (int w = threadIdx.x; w < (int)(sizeof(MemberDesc<T>) / sizeof(int)); w += 32) dst[w] = __ldg(src + w);
+      __syncwarp();
+      const int* gsrc = reinterpret_cast<const int*>(a.geos + ctx.d.geo);
+      int* gdst = reinterpret_cast<int*>(&ctx.g);
+      for (int w = threadIdx.x; w < (int)(sizeof(Geo<T>) / sizeof(int)); w += 32) gdst[w] = __ldg(gsrc + w);
+      __syncwarp();
     }
+    if (threadIdx.x == 0) ctx.io = member_stage(ctx.d, a.rk, step, st);
   }
-  if (threadIdx.x == 0) ctx.io = member_stage(a.mem[k], a.rk, step, st);
   __syncthreads();
   ctx.k = k;
 }
@@ -101,16 +125,27 @@ __device__ __forceinline__ int active_members(const BatchArgs<T>& a, int act, in
   return act;
 }
 
+// Resident CTAs per SM of the batched phase kernels: their member geometry and
+// stage pointers live in shared memory, so the pointers occupy registers; 3
+// CTAs (85 registers) measured faster than 4 (spills) or 2 (occupancy).
+constexpr int kBatchPhaseBlocks = 3;
+
 // Tile phase of every active member (one launch per phase): blockIdx.x is the
 // tile in the member-major tile list.
 template <typename T, int TI, int TJ, bool UV>
-__global__ void __launch_bounds__(kTileThreads) k_batch_phase(BatchArgs<T> a, int step, int st, int act) {
+__global__ void __launch_bounds__(kTileThreads, kBatchPhaseBlocks) k_batch_phase(BatchArgs<T> a, int step, int st, int act) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ TileCtx<T> ctx;
   release_dependents();
   const int tile = blockIdx.x;
-  const int k = member_of(a.off.tile, act, tile);
+  __shared__ int s_k;
+  if (threadIdx.x < 32) {
+    const int k = member_of_warp(a.off.tile, act, tile);
+    if (threadIdx.x == 0) s_k = k;
+  }
   ctx.k = -1;
+  __syncthreads();
+  const int k = s_k;
   ctx_load(ctx, a, k, step, st);
   const Geo<T>& g = ctx.g;
   const TileBox b = tile_box(make_tiling_dev(TI, TJ, g.n), g.n, tile - __ldg(a.off.tile + k));

@@ -22,12 +22,6 @@ namespace bt {
 
 constexpr int kThreads = kTileThreads;
 
-// Resident CTAs per SM the phase kernels are compiled for (register cap
-// 65536 / (256 * blocks)): float64 tiles need more registers per thread.
-template <typename T>
-struct PhaseBlocks {
-  static constexpr int value = sizeof(T) == 8 ? 3 : 4;
-};
 
 template <typename T, int TI, int TJ>
 __global__ void __launch_bounds__(kThreads, PhaseBlocks<T>::value) k_phase_h(Geo<T> g, StageIO<T> io, Tiling t) {

@@ -206,6 +206,13 @@ __device__ __forceinline__ int yface_side(int j, int m) {
 // cp.async in a prologue that does not depend on the state.
 constexpr int kTileThreads = 256;
 
+// Resident CTAs per SM the tile-phase kernels are compiled for (register cap
+// 65536 / (256 * blocks)): float64 tiles need more registers per thread.
+template <typename T>
+struct PhaseBlocks {
+  static constexpr int value = sizeof(T) == 8 ? 3 : 4;
+};
+
 constexpr int up4(int x) { return (x + 3) & ~3; }  // shared-memory offsets in words, 16-byte aligned
 
 template <int TI, int TJ>
