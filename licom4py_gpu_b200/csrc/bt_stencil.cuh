@@ -242,10 +242,12 @@ struct TileShape {
                        hNP = up4(hRDA + C), hNH = hNP + 6 * NE, hNDZ = hNH + 6 * NE, kWordsH = up4(hNDZ + NE);
   static constexpr int hP = hG, hQ = hG + FX;
   static_assert(FX + FY <= 4 * NP, "face fluxes must fit in the metric block they alias");
-  // phase UV (words): s_v [VB], s_u [TI][RJ], s_hn [RI][RJ], cells g [C][4], sina,
+  // phase UV (words): s_v [VB], s_u [TI][RJ], s_hn [RI][RJ], s_hb [RI][RJ] (stage h of
+  // the fb blend, RK3), cells g [C][4], sina,
   // rda, rdx, rdy, a_f; x faces cache [3][FX], c_dy, kinetic energy, v_t * c_dy;
   // y faces cache [3][FY], d_dx, kinetic energy, u_t * d_dx
-  static constexpr int uV = 0, uU = up4(uV + VB), uHN = up4(uU + TI * RJ), uG = up4(uHN + RI * RJ),
+  static constexpr int uV = 0, uU = up4(uV + VB), uHN = up4(uU + TI * RJ), uHB = up4(uHN + RI * RJ),
+                       uG = up4(uHB + RI * RJ),
                        uSN = up4(uG + 4 * C), uRDA = uSN + C, uRDX = uRDA + C, uRDY = uRDX + C, uAF = uRDY + C,
                        uXC = up4(uAF + C), uCDY = up4(uXC + 3 * FX), uKU = up4(uCDY + FX), uVX = up4(uKU + FX),
                        uYC = up4(uVX + FX), uDDX = up4(uYC + 3 * FY), uKV = up4(uDDX + FY), uUY = up4(uKV + FY),
@@ -867,12 +869,13 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
 template <typename T, int TI, int TJ>
 struct LayoutUV {
   using S = TileShape<TI, TJ>;
-  T *s_v, *s_u, *s_hn, *s_g, *s_sn, *s_rda, *s_rdx, *s_rdy, *s_af, *s_xc, *s_cdy, *s_ku, *s_vx, *s_yc, *s_ddx,
-      *s_kv, *s_uy;
+  T *s_v, *s_u, *s_hn, *s_hb, *s_g, *s_sn, *s_rda, *s_rdx, *s_rdy, *s_af, *s_xc, *s_cdy, *s_ku, *s_vx, *s_yc,
+      *s_ddx, *s_kv, *s_uy;
   __device__ __forceinline__ explicit LayoutUV(T* sm) {
     s_v = sm + S::uV;
     s_u = sm + S::uU;
     s_hn = sm + S::uHN;
+    s_hb = sm + S::uHB;
     s_g = sm + S::uG;
     s_sn = sm + S::uSN;
     s_rda = sm + S::uRDA;
@@ -978,50 +981,53 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
     cp_async_t(L.s_yc + 2 * S::FY + e, src + 2 * PF);
   }
 
-  // state of the thread's interior region points and base velocities of its cells
-  T hnv[S::KV], vvv[S::KV], uvv[S::KV], upc[S::KC], vpc[S::KC];
-  T hns = T(0.0), us = T(0.0);
+  // state of the region: interior points by cp.async straight into shared
+  // memory (new h, raw v on the vertical bar, raw u on the tile rows and side
+  // points, the stage h of the fb blend when beta != 0); halo points that no
+  // gather item covers are fetched point by point and stored blended
+  T upc[S::KC], vpc[S::KC];
   const EdgeCover ec(b, m);
   const int ov = cell32(f, b.i0 - kHalo, b.j0 + q, m);
 #pragma unroll
   for (int k = 0; k < S::KV; ++k) {
     const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
     if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
-      T hn, h = T(0.0), u = T(0.0), v;
+      const bool row = r >= kHalo && r < b.ni + kHalo;
+      const int e = r * RJ + q + kHalo;
       if (i >= kHalo && i < m - kHalo) {
         const int o = ov + r * m;
-        hn = hn_src[o];
-        if (blend) h = io.h[o];
-        v = io.v[o];
-        if (r >= kHalo && r < b.ni + kHalo) u = io.u[o];
-      } else {  // uncovered halo row: fetched point by point (the new h never has a stored halo)
-        hn = fetch_s(hn_src, g, f, i, b.j0 + q, 0);
-        if (blend) h = fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
+        cp_async_t(L.s_hn + e, hn_src + o);
+        if (blend) cp_async_t(L.s_hb + e, io.h + o);
+        cp_async_t(L.s_v + r * TJ + q, io.v + o);
+        if (row) cp_async_t(L.s_u + (r - kHalo) * RJ + q + kHalo, io.u + o);
+      } else {  // the new h never has a stored halo
+        T hn = fetch_s(hn_src, g, f, i, b.j0 + q, 0), u, v;
         fetch_v(io.u, io.v, g, f, i, b.j0 + q, io.stored_halo, u, v);
+        if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
+        L.s_hn[e] = hn;
+        L.s_v[r * TJ + q] = v;
+        if (row) L.s_u[(r - kHalo) * RJ + q + kHalo] = u;
       }
-      if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * h;  // fb_scheme, barotr_pure.py:52-54
-      hnv[k] = hn;
-      vvv[k] = v;
-      uvv[k] = u;
     }
   }
   const int t6 = threadIdx.x;
   const int sr = t6 / 6, sc = t6 - 6 * sr, scc = sc < 3 ? sc : b.nj + sc, sj = b.j0 - kHalo + scc;
   const bool side_pt = t6 < 6 * b.ni && ec.col_staged(sj, m);
+  const bool side_in = sj >= kHalo && sj < m - kHalo;
   if (side_pt) {
-    T hn, h = T(0.0), v;
-    if (sj >= kHalo && sj < m - kHalo) {
+    const int e = (sr + kHalo) * RJ + scc;
+    if (side_in) {
       const int o = cell32(f, b.i0 + sr, sj, m);
-      hn = hn_src[o];
-      if (blend) h = io.h[o];
-      us = io.u[o];
+      cp_async_t(L.s_hn + e, hn_src + o);
+      if (blend) cp_async_t(L.s_hb + e, io.h + o);
+      cp_async_t(L.s_u + sr * RJ + scc, io.u + o);
     } else {
-      hn = fetch_s(hn_src, g, f, b.i0 + sr, sj, 0);
-      if (blend) h = fetch_s(io.h, g, f, b.i0 + sr, sj, io.stored_halo);
-      fetch_v(io.u, io.v, g, f, b.i0 + sr, sj, io.stored_halo, us, v);
+      T hn = fetch_s(hn_src, g, f, b.i0 + sr, sj, 0), u, v;
+      fetch_v(io.u, io.v, g, f, b.i0 + sr, sj, io.stored_halo, u, v);
+      if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * fetch_s(io.h, g, f, b.i0 + sr, sj, io.stored_halo);
+      L.s_hn[e] = hn;
+      L.s_u[sr * RJ + scc] = u;
     }
-    if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * h;
-    hns = hn;
   }
 #pragma unroll
   for (int k = 0; k < S::KC; ++k) {
@@ -1032,21 +1038,23 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
     }
   }
   if (P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr});
-#pragma unroll
-  for (int k = 0; k < S::KV; ++k) {
-    const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
-      L.s_hn[r * RJ + q + kHalo] = hnv[k];
-      L.s_v[r * TJ + q] = vvv[k];
-      if (r >= kHalo && r < b.ni + kHalo) L.s_u[(r - kHalo) * RJ + q + kHalo] = uvv[k];
-    }
-  }
-  if (side_pt) {
-    L.s_hn[(sr + kHalo) * RJ + scc] = hns;
-    L.s_u[sr * RJ + scc] = us;
-  }
   cp_async_wait_all();
   __syncthreads();
+  if (blend) {  // fb_scheme, barotr_pure.py:52-54, on the points staged by cp.async
+#pragma unroll
+    for (int k = 0; k < S::KV; ++k) {
+      const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
+      if (q < b.nj && r < b.ni + 6 && i >= kHalo && i < m - kHalo) {
+        const int e = r * RJ + q + kHalo;
+        L.s_hn[e] = (T(1.0) - io.beta) * L.s_hn[e] + io.beta * L.s_hb[e];
+      }
+    }
+    if (side_pt && side_in) {
+      const int e = (sr + kHalo) * RJ + scc;
+      L.s_hn[e] = (T(1.0) - io.beta) * L.s_hn[e] + io.beta * L.s_hb[e];
+    }
+    __syncthreads();
+  }
 
   // faces: upwind tangential component (remap.py:73-95) and kinetic energy (barotr_pure.py:91-92)
   if (q < b.nj) {
