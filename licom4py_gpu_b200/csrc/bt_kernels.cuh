@@ -43,47 +43,53 @@ __global__ void __launch_bounds__(kThreads, PhaseBlocks<T>::value) k_phase_uv(Ge
 // walks its tiles of a phase, then all CTAs meet at a grid barrier.  Before
 // waiting at the barrier a CTA already issues the next phase's prologue for
 // its first tile (constants by cp.async, halo descriptors), so those loads
-// overlap the barrier.
+// overlap the barrier.  The loop runs per RK stage (phase H, barrier, phase
+// UV, barrier) so the two phases' gather states are never live together.
 template <typename T, int TI, int TJ>
 __global__ void __launch_bounds__(kThreads, 3) k_round(RoundArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ StageIO<T> s_io[2];  // stage pointers, alternating between consecutive stages
   T* sm = reinterpret_cast<T*>(smraw);
   const int ntiles = 6 * a.t.tiles_per_face();
   const int nst = a.rk == 2 ? 2 : 3;
-  const int nphase = a.nbb * nst * 2;
+  const int nstage = a.nbb * nst;
   const int t0 = blockIdx.x;
   unsigned gen = 0;
-  Gather<T, TI, TJ, false> gh;
-  Gather<T, TI, TJ, true> gu;
   int cnt[4], P = 0;
-  if (t0 < ntiles) tile_h_pro<T, TI, TJ>(a.g, round_stage(a, 0, 0), tile_box(a.t, a.g.n, t0), sm, gh, cnt, P);
-  for (int ph = 0; ph < nphase; ++ph) {
-    const int step = ph / (2 * nst), st = (ph >> 1) % nst;
-    const bool uv = ph & 1;
-    const StageIO<T> io = round_stage(a, step, st);
+  if (threadIdx.x == 0) s_io[0] = round_stage(a, 0, 0);
+  __syncthreads();
+  // phase H of stage 0: the first tile's prologue
+  Gather<T, TI, TJ, false> gh;
+  if (t0 < ntiles) tile_h_pro<T, TI, TJ>(a.g, s_io[0], tile_box(a.t, a.g.n, t0), sm, gh, cnt, P);
+  for (int sg = 0; sg < nstage; ++sg) {
+    const StageIO<T>& io = s_io[sg & 1];
     int k = 0;
     for (int tile = t0; tile < ntiles; tile += gridDim.x, ++k) {
       const TileBox b = tile_box(a.t, a.g.n, tile);
-      if (!uv) {
-        if (k > 0) tile_h_pro<T, TI, TJ>(a.g, io, b, sm, gh, cnt, P);
-        tile_h_main<T, TI, TJ>(a.g, io, b, sm, gh, cnt, P);
-      } else {
-        if (k > 0) tile_uv_pro<T, TI, TJ>(a.g, io, b, sm, gu, cnt, P);
-        tile_uv_main<T, TI, TJ>(a.g, io, b, sm, gu, cnt, P);
-      }
+      if (k > 0) tile_h_pro<T, TI, TJ>(a.g, io, b, sm, gh, cnt, P);
+      tile_h_main<T, TI, TJ>(a.g, io, b, sm, gh, cnt, P);
       __syncthreads();
     }
-    if (ph + 1 < nphase && t0 < ntiles) {
-      const int nx = ph + 1, nstep = nx / (2 * nst), nst2 = (nx >> 1) % nst;
-      const StageIO<T> io_n = round_stage(a, nstep, nst2);
-      const TileBox b = tile_box(a.t, a.g.n, t0);
-      if (nx & 1)
-        tile_uv_pro<T, TI, TJ>(a.g, io_n, b, sm, gu, cnt, P);
-      else
-        tile_h_pro<T, TI, TJ>(a.g, io_n, b, sm, gh, cnt, P);
-    }
+    Gather<T, TI, TJ, true> gu;
+    if (t0 < ntiles) tile_uv_pro<T, TI, TJ>(a.g, io, tile_box(a.t, a.g.n, t0), sm, gu, cnt, P);
     if (!grid_barrier(a.bar, gen, a.err, a.spin_limit)) {
       cp_async_wait_all();  // no copy may be left in flight when the CTA leaves
+      return;
+    }
+    k = 0;
+    for (int tile = t0; tile < ntiles; tile += gridDim.x, ++k) {
+      const TileBox b = tile_box(a.t, a.g.n, tile);
+      if (k > 0) tile_uv_pro<T, TI, TJ>(a.g, io, b, sm, gu, cnt, P);
+      tile_uv_main<T, TI, TJ>(a.g, io, b, sm, gu, cnt, P);
+      __syncthreads();
+    }
+    if (sg + 1 < nstage) {
+      if (threadIdx.x == 0) s_io[(sg + 1) & 1] = round_stage(a, (sg + 1) / nst, (sg + 1) % nst);
+      __syncthreads();
+      if (t0 < ntiles) tile_h_pro<T, TI, TJ>(a.g, s_io[(sg + 1) & 1], tile_box(a.t, a.g.n, t0), sm, gh, cnt, P);
+    }
+    if (!grid_barrier(a.bar, gen, a.err, a.spin_limit)) {
+      cp_async_wait_all();
       return;
     }
   }

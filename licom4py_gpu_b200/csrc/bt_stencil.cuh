@@ -1198,23 +1198,23 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* 
 }
 
 // Stage pointers of (substep, stage) of a round; mirrors the host schedule.
+// Fields are picked with constant indexes only, so the kernel arguments are
+// never addressed (which would copy them to local memory).
 template <typename T>
-__device__ StageIO<T> round_stage(const RoundArgs<T>& a, int step, int st) {
+__device__ __forceinline__ StageIO<T> round_stage(const RoundArgs<T>& a, int step, int st) {
   StageIO<T> io;
-  const T* const* cur = step == 0 ? a.x0 : (const T* const*)a.x;
-  const T* const* base = step == 0 ? a.b0 : (const T* const*)a.x;
   const int nst = a.rk == 2 ? 2 : 3;
-  const T* const* in = st == 0 ? cur : (st == 1 ? (const T* const*)a.y : (const T* const*)a.z);
-  T* const* out = st == nst - 1 ? a.x : (st == 0 ? a.y : a.z);
-  io.h = in[0];
-  io.u = in[1];
-  io.v = in[2];
-  io.hp = base[0];
-  io.up = base[1];
-  io.vp = base[2];
-  io.h_out = out[0];
-  io.u_out = out[1];
-  io.v_out = out[2];
+  const bool first = step == 0, last = st == nst - 1;
+  // stage input: the round input (first substep) or the running state, then Y, then Z
+  io.h = st == 0 ? (first ? a.x0[0] : a.x[0]) : (st == 1 ? a.y[0] : a.z[0]);
+  io.u = st == 0 ? (first ? a.x0[1] : a.x[1]) : (st == 1 ? a.y[1] : a.z[1]);
+  io.v = st == 0 ? (first ? a.x0[2] : a.x[2]) : (st == 1 ? a.y[2] : a.z[2]);
+  io.hp = first ? a.b0[0] : a.x[0];
+  io.up = first ? a.b0[1] : a.x[1];
+  io.vp = first ? a.b0[2] : a.x[2];
+  io.h_out = last ? a.x[0] : (st == 0 ? a.y[0] : a.z[0]);
+  io.u_out = last ? a.x[1] : (st == 0 ? a.y[1] : a.z[1]);
+  io.v_out = last ? a.x[2] : (st == 0 ? a.y[2] : a.z[2]);
   io.fx = a.fx;
   io.fy = a.fy;
   double dt;
@@ -1226,8 +1226,8 @@ __device__ StageIO<T> round_stage(const RoundArgs<T>& a, int step, int st) {
     io.beta = T(1.0);
   }
   io.dt = (T)dt;
-  io.stored_halo = (step == 0 && st == 0) ? 1 : 0;
-  io.last = st == nst - 1 ? 1 : 0;
+  io.stored_halo = (first && st == 0) ? 1 : 0;
+  io.last = last ? 1 : 0;
   return io;
 }
 
