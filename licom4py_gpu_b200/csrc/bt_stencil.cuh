@@ -271,6 +271,15 @@ __device__ __forceinline__ TileBox tile_box(const Tiling& t, int n, int tile) {
   return b;
 }
 
+// A full interior tile: TI x TJ cells whose whole stencil region (3 cells
+// beyond each side) lies inside the face.  Such a tile needs no halo gather,
+// no edge average and no bounds checks, so the tile phases are compiled
+// separately for it (FULL = true) with its extents as constants.
+__device__ __forceinline__ bool tile_full(const TileBox& b, int m, int ti, int tj) {
+  return b.ni == ti && b.nj == tj && b.i0 >= 2 * kHalo && b.i0 + b.ni + kHalo <= m - kHalo &&
+         b.j0 >= 2 * kHalo && b.j0 + b.nj + kHalo <= m - kHalo;
+}
+
 // 32-bit offset of cell (i, j) of face f (fields of up to 2^31 elements).
 __device__ __forceinline__ int cell32(int f, int i, int j, int m) { return (f * m + i) * m + j; }
 
@@ -634,38 +643,39 @@ struct LayoutH {
 // Phase H prologue: constants of the tile (cp.async, not yet awaited) and the
 // halo-gather descriptors.  Independent of the state, so it may run before the
 // previous phase has finished (programmatic launch, or before a grid barrier).
-template <typename T, int TI, int TJ>
-__device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                           Gather<T, TI, TJ, false>& gat, int* cnt, int& P) {
+template <typename T, int TI, int TJ, bool FULL>
+__device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                             Gather<T, TI, TJ, false>& gat, int* cnt, int& P) {
   using S = TileShape<TI, TJ>;
   const LayoutH<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
+  const int ni = FULL ? TI : b.ni, nj = FULL ? TJ : b.nj;
   // region metric (halo points of edge tiles are also read by the gather items, from global memory)
-  if (q < b.nj) {
+  if (q < nj) {
     const int o0 = cell32(b.f, b.i0 - kHalo, b.j0 + q, m);
 #pragma unroll
     for (int k = 0; k < S::KV; ++k) {
       const int r = sl + k * S::NS;
-      if (r < b.ni + 6) {
+      if (r < ni + 6) {
         const int o = o0 + r * m, p = r * TJ + q;
         cp_async_mat(L.s_g + 4 * p, g.gct + 4 * (long)o);
         cp_async_t(L.s_sn + p, g.sina + o);
       }
     }
   }
-  if (threadIdx.x < 6 * b.ni) {
-    const int t = threadIdx.x, r = t / 6, c = t - 6 * r, cc = c < 3 ? c : b.nj + c;
+  if (threadIdx.x < 6 * ni) {
+    const int t = threadIdx.x, r = t / 6, c = t - 6 * r, cc = c < 3 ? c : nj + c;
     const int o = cell32(b.f, b.i0 + r, b.j0 - kHalo + cc, m), p = S::VB + t;
     cp_async_mat(L.s_g + 4 * p, g.gct + 4 * (long)o);
     cp_async_t(L.s_sn + p, g.sina + o);
   }
   // face and cell constants
-  if (q < b.nj) {
+  if (q < nj) {
     const int o0 = cell32(b.f, b.i0, b.j0 + q, m);
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
       const int a = sl + k * S::NS;
-      if (a <= b.ni) {
+      if (a <= ni) {
         cp_async_t(L.s_dzx + a * TJ + q, g.dzph_x + o0 + a * m);
         cp_async_t(L.s_cdy + a * TJ + q, g.c_dy + o0 + a * m);
       }
@@ -673,27 +683,31 @@ __device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io
 #pragma unroll
     for (int k = 0; k < S::KC; ++k) {
       const int a = sl + k * S::NS;
-      if (a < b.ni) cp_async_t(L.s_rda + a * TJ + q, g.rda + o0 + a * m);
+      if (a < ni) cp_async_t(L.s_rda + a * TJ + q, g.rda + o0 + a * m);
     }
   }
-  if (q <= b.nj) {
+  if (q <= nj) {
     const int o0 = cell32(b.f, b.i0, b.j0 + q, m);
 #pragma unroll
     for (int k = 0; k < S::KC; ++k) {
       const int r = sl + k * S::NS;
-      if (r < b.ni) {
+      if (r < ni) {
         cp_async_t(L.s_dzy + r * (TJ + 1) + q, g.dzph_y + o0 + r * m);
         cp_async_t(L.s_ddx + r * (TJ + 1) + q, g.d_dx + o0 + r * m);
       }
     }
   }
-  if (b.nj == TJ && east_row() >= 0 && east_row() < b.ni) {  // the last y-face column of full-width tiles
+  if (nj == TJ && east_row() >= 0 && east_row() < ni) {  // the last y-face column of full-width tiles
     const int r = east_row(), o = cell32(b.f, b.i0 + r, b.j0 + TJ, m);
     cp_async_t(L.s_dzy + r * (TJ + 1) + TJ, g.dzph_y + o);
     cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + o);
   }
-  P = edge_count(b, m, cnt);
-  if (P > 0) gat.descriptors(g, io, b, cnt, P);
+  if (FULL) {
+    P = 0;
+  } else {
+    P = edge_count(b, m, cnt);
+    if (P > 0) gat.descriptors(g, io, b, cnt, P);
+  }
 }
 
 // Phase H of one x face or y face: C-grid normal velocity (remap.py:41-55)
@@ -737,13 +751,14 @@ __device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, c
 }
 
 // Phase H of one tile: writes the new h on the tile's interior cells.
-template <typename T, int TI, int TJ>
-__device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                            Gather<T, TI, TJ, false>& gat, const int* cnt, int P) {
+template <typename T, int TI, int TJ, bool FULL>
+__device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                              Gather<T, TI, TJ, false>& gat, const int* cnt, int P) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
   static_assert(6 * TI <= kTileThreads, "one side point per thread");
   const int m = g.m, n = g.n, f = b.f, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
+  const int ni = FULL ? TI : b.ni, nj = FULL ? TJ : b.nj;
   const LayoutH<T, TI, TJ> L(sm);
   // state of the thread's interior region points and base h of its cells, into registers
   T hv[S::KV], uv[S::KV], vv[S::KV], hpc[S::KC];
@@ -753,8 +768,8 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
 #pragma unroll
   for (int k = 0; k < S::KV; ++k) {
     const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
-      if (i >= kHalo && i < m - kHalo) {
+    if (q < nj && r < ni + 6 && (FULL || ec.row_staged(i, m))) {
+      if (FULL || (i >= kHalo && i < m - kHalo)) {
         const int o = ov + r * m;
         hv[k] = io.h[o];
         uv[k] = io.u[o];
@@ -766,10 +781,10 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
     }
   }
   const int t6 = threadIdx.x;
-  const int sr = t6 / 6, sc = t6 - 6 * sr, scc = sc < 3 ? sc : b.nj + sc, sj = b.j0 - kHalo + scc;
-  const bool side_pt = t6 < 6 * b.ni && ec.col_staged(sj, m);
+  const int sr = t6 / 6, sc = t6 - 6 * sr, scc = sc < 3 ? sc : nj + sc, sj = b.j0 - kHalo + scc;
+  const bool side_pt = t6 < 6 * ni && (FULL || ec.col_staged(sj, m));
   if (side_pt) {
-    if (sj >= kHalo && sj < m - kHalo) {
+    if (FULL || (sj >= kHalo && sj < m - kHalo)) {
       const int o = cell32(f, b.i0 + sr, sj, m);
       hs = io.h[o];
       us = io.u[o];
@@ -782,9 +797,9 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
 #pragma unroll
   for (int k = 0; k < S::KC; ++k) {
     const int a = sl + k * S::NS;
-    if (q < b.nj && a < b.ni) hpc[k] = io.hp[ov + (a + kHalo) * m];
+    if (q < nj && a < ni) hpc[k] = io.hp[ov + (a + kHalo) * m];
   }
-  if (P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_h, L.s_uc, L.s_vc, L.s_np, L.s_nh, L.s_ndz});
+  if (!FULL && P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_h, L.s_uc, L.s_vc, L.s_np, L.s_nh, L.s_ndz});
   cp_async_wait_all();
   __syncthreads();
 
@@ -792,13 +807,13 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
 #pragma unroll
   for (int k = 0; k < S::KV; ++k) {
     const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
+    if (q < nj && r < ni + 6 && (FULL || ec.row_staged(i, m))) {
       const int p = r * TJ + q;
       const T* G = L.s_g + 4 * p;
       const T sn = L.s_sn[p], u = uv[k], v = vv[k];
       L.s_h[r * RJ + q + kHalo] = hv[k];
       L.s_uc[p] = (G[0] * u + G[1] * v) * sn;
-      if (r >= kHalo && r < b.ni + kHalo) L.s_vc[(r - kHalo) * RJ + q + kHalo] = (G[2] * u + G[3] * v) * sn;
+      if (r >= kHalo && r < ni + kHalo) L.s_vc[(r - kHalo) * RJ + q + kHalo] = (G[2] * u + G[3] * v) * sn;
     }
   }
   if (side_pt) {
@@ -811,14 +826,15 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
 
   // faces; their fluxes (times c_dy / d_dx) alias the metric block, no longer read
   const int PF = 6 * (n + 1) * n;  // plane size of both face caches
-  if (q < b.nj) {
+  if (q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
       const int a = sl + k * S::NS;
-      if (a <= b.ni) {
-        const int side = (a == 0 && b.i0 == kHalo) ? kS : ((a == b.ni && b.i0 + b.ni == m - kHalo) ? kN : -1);
+      if (a <= ni) {
+        const int side =
+            FULL ? -1 : ((a == 0 && b.i0 == kHalo) ? kS : ((a == ni && b.i0 + ni == m - kHalo) ? kN : -1));
         const int e = a * TJ + q;
-        T* fc = (a < b.ni || side == kN)
+        T* fc = (a < ni || side == kN)
                     ? io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n)
                     : nullptr;
         const T fl = face_h<T>(io, L.s_h + a * RJ + q + kHalo, RJ, L.s_uc + a * TJ + q, TJ, side,
@@ -834,15 +850,16 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
     if (k < S::KC) {
       r = sl + k * S::NS;
       qq = q;
-      if (r >= b.ni || q > b.nj) continue;
+      if (r >= ni || q > nj) continue;
     } else {
       r = east_row();
       qq = TJ;
-      if (b.nj != TJ || r < 0 || r >= b.ni) continue;
+      if (nj != TJ || r < 0 || r >= ni) continue;
     }
-    const int side = (qq == 0 && b.j0 == kHalo) ? kW : ((qq == b.nj && b.j0 + b.nj == m - kHalo) ? kE : -1);
+    const int side =
+        FULL ? -1 : ((qq == 0 && b.j0 == kHalo) ? kW : ((qq == nj && b.j0 + nj == m - kHalo) ? kE : -1));
     const int e = r * (TJ + 1) + qq;
-    T* fc = (qq < b.nj || side == kE)
+    T* fc = (qq < nj || side == kE)
                 ? io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n)
                 : nullptr;
     const T fl = face_h<T>(io, L.s_h + (r + kHalo) * RJ + qq, 1, L.s_vc + r * RJ + qq, 1, side,
@@ -852,11 +869,11 @@ __device__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox
   __syncthreads();
 
   // cells: divergence (agrid.py:43-53) and the h update (barotr_pure.py:119-120)
-  if (q < b.nj) {
+  if (q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KC; ++k) {
       const int a = sl + k * S::NS;
-      if (a < b.ni) {
+      if (a < ni) {
         const int x0 = a * TJ + q, y0 = a * (TJ + 1) + q;
         const T div = L.s_rda[x0] * (L.s_P[x0 + TJ] - L.s_P[x0] + L.s_Q[y0 + 1] - L.s_Q[y0]);
         io.h_out[ov + (a + kHalo) * m] = hpc[k] - div * io.dt;
@@ -894,18 +911,19 @@ struct LayoutUV {
 };
 
 // Phase UV prologue: cell and face constants (cp.async) and the halo-gather descriptors.
-template <typename T, int TI, int TJ>
-__device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                            Gather<T, TI, TJ, true>& gat, int* cnt, int& P) {
+template <typename T, int TI, int TJ, bool FULL>
+__device__ __forceinline__ void tile_uv_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                              Gather<T, TI, TJ, true>& gat, int* cnt, int& P) {
   using S = TileShape<TI, TJ>;
   const LayoutUV<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
+  const int ni = FULL ? TI : b.ni, nj = FULL ? TJ : b.nj;
   const int o0 = cell32(b.f, b.i0, b.j0 + q, m);
-  if (q < b.nj) {
+  if (q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KC; ++k) {
       const int a = sl + k * S::NS;
-      if (a < b.ni) {
+      if (a < ni) {
         const int o = o0 + a * m, e = a * TJ + q;
         cp_async_mat(L.s_g + 4 * e, g.gct + 4 * (long)o);
         cp_async_t(L.s_sn + e, g.sina + o);
@@ -918,42 +936,47 @@ __device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& i
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
       const int a = sl + k * S::NS;
-      if (a <= b.ni) cp_async_t(L.s_cdy + a * TJ + q, g.c_dy + o0 + a * m);
+      if (a <= ni) cp_async_t(L.s_cdy + a * TJ + q, g.c_dy + o0 + a * m);
     }
   }
-  if (q <= b.nj) {
+  if (q <= nj) {
 #pragma unroll
     for (int k = 0; k < S::KC; ++k) {
       const int r = sl + k * S::NS;
-      if (r < b.ni) cp_async_t(L.s_ddx + r * (TJ + 1) + q, g.d_dx + o0 + r * m);
+      if (r < ni) cp_async_t(L.s_ddx + r * (TJ + 1) + q, g.d_dx + o0 + r * m);
     }
   }
-  if (b.nj == TJ && east_row() >= 0 && east_row() < b.ni) {
+  if (nj == TJ && east_row() >= 0 && east_row() < ni) {
     const int r = east_row();
     cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + cell32(b.f, b.i0 + r, b.j0 + TJ, m));
   }
-  P = edge_count(b, m, cnt);
-  if (P > 0) gat.descriptors(g, io, b, cnt, P);
+  if (FULL) {
+    P = 0;
+  } else {
+    P = edge_count(b, m, cnt);
+    if (P > 0) gat.descriptors(g, io, b, cnt, P);
+  }
 }
 
-template <typename T, int TI, int TJ>
-__device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                             Gather<T, TI, TJ, true>& gat, const int* cnt, int P) {
+template <typename T, int TI, int TJ, bool FULL>
+__device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                               Gather<T, TI, TJ, true>& gat, const int* cnt, int P) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
   static_assert(6 * TI <= kTileThreads, "one side point per thread");
   const int m = g.m, n = g.n, f = b.f, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
+  const int ni = FULL ? TI : b.ni, nj = FULL ? TJ : b.nj;
   const LayoutUV<T, TI, TJ> L(sm);
   const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
   const T* hn_src = (const T*)io.h_out;
   const int PF = 6 * (n + 1) * n;
 
   // face caches of this stage (written by phase H) -> shared memory
-  if (q < b.nj) {
+  if (q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
       const int a = sl + k * S::NS;
-      if (a <= b.ni) {
+      if (a <= ni) {
         const T* src = io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n);
         const int e = a * TJ + q;
         cp_async_t(L.s_xc + e, src);
@@ -968,11 +991,11 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
     if (k < S::KC) {
       r = sl + k * S::NS;
       qq = q;
-      if (r >= b.ni || q > b.nj) continue;
+      if (r >= ni || q > nj) continue;
     } else {
       r = east_row();
       qq = TJ;
-      if (b.nj != TJ || r < 0 || r >= b.ni) continue;
+      if (nj != TJ || r < 0 || r >= ni) continue;
     }
     const T* src = io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n);
     const int e = r * (TJ + 1) + qq;
@@ -991,10 +1014,10 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
 #pragma unroll
   for (int k = 0; k < S::KV; ++k) {
     const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-    if (q < b.nj && r < b.ni + 6 && ec.row_staged(i, m)) {
-      const bool row = r >= kHalo && r < b.ni + kHalo;
+    if (q < nj && r < ni + 6 && (FULL || ec.row_staged(i, m))) {
+      const bool row = r >= kHalo && r < ni + kHalo;
       const int e = r * RJ + q + kHalo;
-      if (i >= kHalo && i < m - kHalo) {
+      if (FULL || (i >= kHalo && i < m - kHalo)) {
         const int o = ov + r * m;
         cp_async_t(L.s_hn + e, hn_src + o);
         if (blend) cp_async_t(L.s_hb + e, io.h + o);
@@ -1011,9 +1034,9 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
     }
   }
   const int t6 = threadIdx.x;
-  const int sr = t6 / 6, sc = t6 - 6 * sr, scc = sc < 3 ? sc : b.nj + sc, sj = b.j0 - kHalo + scc;
-  const bool side_pt = t6 < 6 * b.ni && ec.col_staged(sj, m);
-  const bool side_in = sj >= kHalo && sj < m - kHalo;
+  const int sr = t6 / 6, sc = t6 - 6 * sr, scc = sc < 3 ? sc : nj + sc, sj = b.j0 - kHalo + scc;
+  const bool side_pt = t6 < 6 * ni && (FULL || ec.col_staged(sj, m));
+  const bool side_in = FULL || (sj >= kHalo && sj < m - kHalo);
   if (side_pt) {
     const int e = (sr + kHalo) * RJ + scc;
     if (side_in) {
@@ -1032,19 +1055,19 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
 #pragma unroll
   for (int k = 0; k < S::KC; ++k) {
     const int a = sl + k * S::NS;
-    if (q < b.nj && a < b.ni) {
+    if (q < nj && a < ni) {
       upc[k] = io.up[ov + (a + kHalo) * m];
       vpc[k] = io.vp[ov + (a + kHalo) * m];
     }
   }
-  if (P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr});
+  if (!FULL && P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr});
   cp_async_wait_all();
   __syncthreads();
   if (blend) {  // fb_scheme, barotr_pure.py:52-54, on the points staged by cp.async
 #pragma unroll
     for (int k = 0; k < S::KV; ++k) {
       const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-      if (q < b.nj && r < b.ni + 6 && i >= kHalo && i < m - kHalo) {
+      if (q < nj && r < ni + 6 && (FULL || (i >= kHalo && i < m - kHalo))) {
         const int e = r * RJ + q + kHalo;
         L.s_hn[e] = (T(1.0) - io.beta) * L.s_hn[e] + io.beta * L.s_hb[e];
       }
@@ -1057,11 +1080,11 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
   }
 
   // faces: upwind tangential component (remap.py:73-95) and kinetic energy (barotr_pure.py:91-92)
-  if (q < b.nj) {
+  if (q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
       const int a = sl + k * S::NS;
-      if (a <= b.ni) {
+      if (a <= ni) {
         const int e = a * TJ + q;
         const T* pt = L.s_v + a * TJ + q;
         T p6[6];
@@ -1080,11 +1103,11 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
     if (k < S::KC) {
       r = sl + k * S::NS;
       qq = q;
-      if (r >= b.ni || q > b.nj) continue;
+      if (r >= ni || q > nj) continue;
     } else {
       r = east_row();
       qq = TJ;
-      if (b.nj != TJ || r < 0 || r >= b.ni) continue;
+      if (nj != TJ || r < 0 || r >= ni) continue;
     }
     const int e = r * (TJ + 1) + qq;
     const T* pt = L.s_u + r * RJ + qq;
@@ -1098,11 +1121,11 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
   }
   __syncthreads();
 
-  if (q < b.nj) {
+  if (q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KC; ++k) {
       const int a = sl + k * S::NS;
-      if (a >= b.ni) continue;
+      if (a >= ni) continue;
       const int e = a * TJ + q;
       const int xf0 = e, xf1 = e + TJ;
       const int yf0 = a * (TJ + 1) + q, yf1 = yf0 + 1;
@@ -1135,6 +1158,42 @@ __device__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBo
       io.v_out[o] = vpc[k] + (pgv + advy - af * uct + visy) * io.dt;
     }
   }
+}
+
+// Tile phases dispatched on the tile's kind: full interior tiles run the
+// FULL = true instantiation.  Prologue and main part of one tile must take
+// the same branch, which they do since both test the same tile box.
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                           Gather<T, TI, TJ, false>& gat, int* cnt, int& P) {
+  if (tile_full(b, g.m, TI, TJ))
+    tile_h_pro_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
+  else
+    tile_h_pro_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
+}
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                            Gather<T, TI, TJ, false>& gat, const int* cnt, int P) {
+  if (tile_full(b, g.m, TI, TJ))
+    tile_h_main_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
+  else
+    tile_h_main_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
+}
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                            Gather<T, TI, TJ, true>& gat, int* cnt, int& P) {
+  if (tile_full(b, g.m, TI, TJ))
+    tile_uv_pro_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
+  else
+    tile_uv_pro_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
+}
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                             Gather<T, TI, TJ, true>& gat, const int* cnt, int P) {
+  if (tile_full(b, g.m, TI, TJ))
+    tile_uv_main_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
+  else
+    tile_uv_main_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
 }
 
 // One tile phase with the prologue issued first (the stream/graph kernels).
