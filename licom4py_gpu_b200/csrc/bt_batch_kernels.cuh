@@ -232,7 +232,8 @@ __global__ void __launch_bounds__(kTileThreads, 2) k_batch_round(BatchArgs<T> a)
       ctx_load(ctx, a, k, step, st);
       const Geo<T>& g = ctx.g;
       const TileBox b = tile_box(make_tiling_dev(TI, TJ, g.n), g.n, tile - __ldg(a.off.tile + k));
-      int cnt[4], P;
+      EdgeCnt cnt;
+      int P;
       if (!uv) {
         Gather<T, TI, TJ, false> gat;
         tile_h_pro<T, TI, TJ>(g, ctx.io, b, sm, gat, cnt, P);

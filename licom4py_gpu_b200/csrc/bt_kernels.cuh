@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_round(RoundArgs<T> a) {
   const int nstage = a.nbb * nst;
   const int t0 = blockIdx.x;
   unsigned gen = 0;
-  int cnt[4], P = 0;
+  EdgeCnt cnt;
+  int P = 0;
   if (threadIdx.x == 0) s_io[0] = round_stage(a, 0, 0);
   __syncthreads();
   // phase H of stage 0: the first tile's prologue

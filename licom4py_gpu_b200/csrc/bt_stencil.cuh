@@ -232,7 +232,7 @@ struct TileShape {
   static constexpr int KV = (RI + NS - 1) / NS;     // row iterations over the vertical bar
   static constexpr int KX = (TI + 1 + NS - 1) / NS; // over x-face rows
   static constexpr int KC = (TI + NS - 1) / NS;     // over tile rows
-  static constexpr int MI = 4;                      // gather items per thread handled in the two-sweep path
+  static constexpr int MI = 2;                      // gather items per thread handled in the two-sweep path
   // phase H (words): s_h [RI][RJ], s_uc [VB], s_vc [TI][RJ], s_g [NP][4], s_sn [NP],
   // s_dzx/s_cdy [FX], s_dzy/s_ddx [FY], s_rda [C], neighbour lines; s_P [FX] and
   // s_Q [FY] alias s_g (dead once the region is staged)
@@ -362,21 +362,38 @@ __device__ __forceinline__ void pull_v(const Pull<T>& p, const Geo<T>& g, const 
 struct EdgeItem {
   int kind, pos, side, k;
 };
-__device__ __forceinline__ int edge_count(const TileBox& b, int m, int* cnt) {
-  cnt[0] = b.i0 == kHalo ? b.nj : 0;
-  cnt[1] = b.i0 + b.ni == m - kHalo ? b.nj : 0;
-  cnt[2] = b.j0 == kHalo ? b.ni : 0;
-  cnt[3] = b.j0 + b.nj == m - kHalo ? b.ni : 0;
-  return cnt[0] + cnt[1] + cnt[2] + cnt[3];
+// Edge positions of a tile per kind (S, N, W, E) and the routes of the
+// tile's face across its four sides (8 bits each, kind order).  Scalars, not
+// arrays: a dynamically indexed array would live in local memory, and each
+// decode would wait on it.
+struct EdgeCnt {
+  int s, n, w, e, routes;
+};
+__device__ __forceinline__ int edge_count(const TileBox& b, int m, const int* route, EdgeCnt& c) {
+  c.s = b.i0 == kHalo ? b.nj : 0;
+  c.n = b.i0 + b.ni == m - kHalo ? b.nj : 0;
+  c.w = b.j0 == kHalo ? b.ni : 0;
+  c.e = b.j0 + b.nj == m - kHalo ? b.ni : 0;
+  c.routes = route[b.f * 4 + kS] | (route[b.f * 4 + kN] << 8) | (route[b.f * 4 + kW] << 16) |
+             (route[b.f * 4 + kE] << 24);
+  return c.s + c.n + c.w + c.e;
 }
-__device__ __forceinline__ EdgeItem edge_item(const TileBox& b, const int* cnt, int q) {
+__device__ __forceinline__ EdgeItem edge_item(const TileBox& b, const EdgeCnt& c, int q) {
   EdgeItem e;
-  int kind = 0;
-  while (q >= cnt[kind]) q -= cnt[kind++];
+  int kind;
+  if (q < c.s) {
+    kind = 0;
+  } else if ((q -= c.s) < c.n) {
+    kind = 1;
+  } else if ((q -= c.n) < c.w) {
+    kind = 2;
+  } else {
+    q -= c.w;
+    kind = 3;
+  }
   e.kind = kind;
   e.pos = q;
-  const int sides[4] = {kS, kN, kW, kE};
-  e.side = sides[kind];
+  e.side = kind == 0 ? kS : (kind == 1 ? kN : (kind == 2 ? kW : kE));
   e.k = kind < 2 ? (b.j0 + q - kHalo) : (b.i0 + q - kHalo);
   return e;
 }
@@ -401,8 +418,8 @@ struct ItemCell {
   int line, y, q;   // line item: 1, normal axis (1 = y), point index
 };
 
-__device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt, int P, int t, int m, int n,
-                                                const int* route, int EW) {
+__device__ __forceinline__ ItemCell decode_item(const TileBox& b, const EdgeCnt& cnt, int P, int t, int m, int n,
+                                                int EW) {
   ItemCell c;
   if (t < 3 * P) {
     const EdgeItem e = edge_item(b, cnt, t / 3);
@@ -428,7 +445,7 @@ __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const int* cnt
     const int t2 = t - 3 * P;
     const EdgeItem e = edge_item(b, cnt, t2 / 6);
     const int q = t2 % 6;
-    const int r = route[b.f * 4 + e.side];
+    const int r = (cnt.routes >> (8 * e.kind)) & 0xff;
     const int ns = route_side(r);
     const int kk = route_rev(r) ? n - 1 - e.k : e.k;
     c.f = route_nb(r);
@@ -470,14 +487,14 @@ struct Gather {
 
   // sweep 1: descriptors of the items' halo gathers (constants, may precede the grid dependency)
   __device__ __forceinline__ void descriptors(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
-                                              const int* cnt, int P) {
+                                              const EdgeCnt& cnt, int P) {
     const int nitems = kPerPos * P;
 #pragma unroll
     for (int k = 0; k < S::MI; ++k) {
       const int t = threadIdx.x + k * kTileThreads;
       pl[k] = false;
       if (t < nitems) {
-        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::EW);
+        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
         if (needs_pull(io, c, g.m)) {
           pd[k] = pull_desc(g, c.f, c.i, c.j);
           pl[k] = true;
@@ -500,13 +517,15 @@ struct Gather {
         pull_v(p, g, io.u, io.v, o, u, v);
       }
       if (!UV) {
-        k.h[c.r * S::RJ + c.c] = direct ? io.h[o] : pull_s(p, io.h);
-        const T* G = g.gct + 4 * o;
-        const T sn = g.sina[o];
+        // every load of the item before its first shared-memory store: one round trip
+        const T h = direct ? io.h[o] : pull_s(p, io.h);
+        const T* G = g.gct + 4 * o + (vert ? 0 : 2);
+        const T ct = (G[0] * u + G[1] * v) * g.sina[o];  // remap.py:34-39
+        k.h[c.r * S::RJ + c.c] = h;
         if (vert)
-          k.vb[c.r * TJ + (c.c - kHalo)] = (G[0] * u + G[1] * v) * sn;  // remap.py:34-39
+          k.vb[c.r * TJ + (c.c - kHalo)] = ct;
         else
-          k.hb[(c.r - kHalo) * S::RJ + c.c] = (G[2] * u + G[3] * v) * sn;
+          k.hb[(c.r - kHalo) * S::RJ + c.c] = ct;
       } else {
         T hn = pull_s(p, (const T*)io.h_out);
         if (io.beta != T(0.0)) {
@@ -530,29 +549,30 @@ struct Gather {
         v = io.v[o];
         if (want_h) h = io.h[o];
       }
+      const T dz = (want_h && c.q == 3) ? (c.y ? g.dzph_y[o] : g.dzph_x[o]) : T(0.0);
       k.np[c.slot] = contra(g, o, u, v, c.y);
       if (want_h) {
         k.nh[c.slot] = h;
-        if (c.q == 3) k.ndz[c.slot / 6] = c.y ? g.dzph_y[o] : g.dzph_x[o];
+        if (c.q == 3) k.ndz[c.slot / 6] = dz;
       }
     }
   }
 
   // sweep 2: sources (state, after the grid dependency) and the items' values
-  __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, const int* cnt,
-                                          int P, const GatherSink<T>& k) {
+  __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
+                                          const EdgeCnt& cnt, int P, const GatherSink<T>& k) {
     const int nitems = kPerPos * P;
 #pragma unroll
     for (int q = 0; q < S::MI; ++q) {
       const int t = threadIdx.x + q * kTileThreads;
       if (t < nitems) {
-        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::EW);
+        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
         one(g, io, c, pd[q], pl[q], k);
       }
     }
     // items beyond MI per thread (only tiles spanning several face edges of tiny faces)
     for (int t = threadIdx.x + S::MI * kTileThreads; t < nitems; t += kTileThreads) {
-      const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, g.route, S::EW);
+      const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
       const bool pull = needs_pull(io, c, g.m);
       Pull<T> p;
       if (pull) p = pull_desc(g, c.f, c.i, c.j);
@@ -645,7 +665,7 @@ struct LayoutH {
 // previous phase has finished (programmatic launch, or before a grid barrier).
 template <typename T, int TI, int TJ, bool FULL>
 __device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                             Gather<T, TI, TJ, false>& gat, int* cnt, int& P) {
+                                             Gather<T, TI, TJ, false>& gat, EdgeCnt& cnt, int& P) {
   using S = TileShape<TI, TJ>;
   const LayoutH<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
@@ -705,7 +725,7 @@ __device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& 
   if (FULL) {
     P = 0;
   } else {
-    P = edge_count(b, m, cnt);
+    P = edge_count(b, m, g.route, cnt);
     if (P > 0) gat.descriptors(g, io, b, cnt, P);
   }
 }
@@ -753,7 +773,7 @@ __device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, c
 // Phase H of one tile: writes the new h on the tile's interior cells.
 template <typename T, int TI, int TJ, bool FULL>
 __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                              Gather<T, TI, TJ, false>& gat, const int* cnt, int P) {
+                                              Gather<T, TI, TJ, false>& gat, const EdgeCnt& cnt, int P) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
   static_assert(6 * TI <= kTileThreads, "one side point per thread");
@@ -913,7 +933,7 @@ struct LayoutUV {
 // Phase UV prologue: cell and face constants (cp.async) and the halo-gather descriptors.
 template <typename T, int TI, int TJ, bool FULL>
 __device__ __forceinline__ void tile_uv_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                              Gather<T, TI, TJ, true>& gat, int* cnt, int& P) {
+                                              Gather<T, TI, TJ, true>& gat, EdgeCnt& cnt, int& P) {
   using S = TileShape<TI, TJ>;
   const LayoutUV<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
@@ -953,14 +973,14 @@ __device__ __forceinline__ void tile_uv_pro_t(const Geo<T>& g, const StageIO<T>&
   if (FULL) {
     P = 0;
   } else {
-    P = edge_count(b, m, cnt);
+    P = edge_count(b, m, g.route, cnt);
     if (P > 0) gat.descriptors(g, io, b, cnt, P);
   }
 }
 
 template <typename T, int TI, int TJ, bool FULL>
 __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                               Gather<T, TI, TJ, true>& gat, const int* cnt, int P) {
+                                               Gather<T, TI, TJ, true>& gat, const EdgeCnt& cnt, int P) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
   static_assert(6 * TI <= kTileThreads, "one side point per thread");
@@ -1165,7 +1185,7 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
 // the same branch, which they do since both test the same tile box.
 template <typename T, int TI, int TJ>
 __device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                           Gather<T, TI, TJ, false>& gat, int* cnt, int& P) {
+                                           Gather<T, TI, TJ, false>& gat, EdgeCnt& cnt, int& P) {
   if (tile_full(b, g.m, TI, TJ))
     tile_h_pro_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
@@ -1173,7 +1193,7 @@ __device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io
 }
 template <typename T, int TI, int TJ>
 __device__ __forceinline__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                            Gather<T, TI, TJ, false>& gat, const int* cnt, int P) {
+                                            Gather<T, TI, TJ, false>& gat, const EdgeCnt& cnt, int P) {
   if (tile_full(b, g.m, TI, TJ))
     tile_h_main_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
@@ -1181,7 +1201,7 @@ __device__ __forceinline__ void tile_h_main(const Geo<T>& g, const StageIO<T>& i
 }
 template <typename T, int TI, int TJ>
 __device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                            Gather<T, TI, TJ, true>& gat, int* cnt, int& P) {
+                                            Gather<T, TI, TJ, true>& gat, EdgeCnt& cnt, int& P) {
   if (tile_full(b, g.m, TI, TJ))
     tile_uv_pro_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
@@ -1189,7 +1209,7 @@ __device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& i
 }
 template <typename T, int TI, int TJ>
 __device__ __forceinline__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                             Gather<T, TI, TJ, true>& gat, const int* cnt, int P) {
+                                             Gather<T, TI, TJ, true>& gat, const EdgeCnt& cnt, int P) {
   if (tile_full(b, g.m, TI, TJ))
     tile_uv_main_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
@@ -1200,7 +1220,8 @@ __device__ __forceinline__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& 
 template <typename T, int TI, int TJ>
 __device__ __forceinline__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
   Gather<T, TI, TJ, false> gat;
-  int cnt[4], P;
+  EdgeCnt cnt;
+  int P;
   tile_h_pro<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
   wait_prior_grid();
   tile_h_main<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
@@ -1208,7 +1229,8 @@ __device__ __forceinline__ void tile_h(const Geo<T>& g, const StageIO<T>& io, co
 template <typename T, int TI, int TJ>
 __device__ __forceinline__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
   Gather<T, TI, TJ, true> gat;
-  int cnt[4], P;
+  EdgeCnt cnt;
+  int P;
   tile_uv_pro<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
   wait_prior_grid();
   tile_uv_main<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
