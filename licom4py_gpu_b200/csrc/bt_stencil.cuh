@@ -503,58 +503,84 @@ struct Gather {
     }
   }
 
+  // One item.  Every lane issues the same loads whatever its item's kind --
+  // the two sources of an interpolated halo value, or the cell itself twice
+  // for a direct read -- so a warp mixing kinds waits for one memory round
+  // trip, not one per kind; the results are selected afterwards (a direct
+  // read stays exact), and all loads precede the item's shared-memory stores.
   __device__ __forceinline__ void one(const Geo<T>& g, const StageIO<T>& io, const ItemCell& c, const Pull<T>& p,
                                       bool pull, const GatherSink<T>& k) {
-    const long o = cell(c.f, c.i, c.j, g.m);
-    if (!c.line) {
-      const bool vert = c.kind < 2;  // S/N halo rows belong to the vertical bar
-      const bool direct = io.stored_halo;
-      T u, v;
-      if (direct) {
-        u = io.u[o];
-        v = io.v[o];
-      } else {
-        pull_v(p, g, io.u, io.v, o, u, v);
+    const int o = cell32(c.f, c.i, c.j, g.m);
+    const bool vpull = UV ? !io.stored_halo : pull;  // velocity interpolated (else read directly)
+    const int sa = vpull ? p.s.x : o, sb = vpull ? p.s.y : o;
+    const T ua = io.u[sa], va = io.v[sa], ub = io.u[sb], vb = io.v[sb];
+    T c0[4], c1[4], l2[4];
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+      c0[z] = g.c2l[4 * (long)sa + z];
+      c1[z] = g.c2l[4 * (long)sb + z];
+      l2[z] = g.l2c[4 * (long)o + z];
+    }
+    if (!UV) {
+      const bool want_h = !c.line || io.last;  // region h, or the neighbour h of the mass-flux average
+      T ha = T(0.0), hb = T(0.0), dz = T(0.0);
+      if (want_h) {
+        ha = io.h[sa];
+        hb = io.h[sb];
       }
-      if (!UV) {
-        // every load of the item before its first shared-memory store: one round trip
-        const T h = direct ? io.h[o] : pull_s(p, io.h);
-        const T* G = g.gct + 4 * o + (vert ? 0 : 2);
-        const T ct = (G[0] * u + G[1] * v) * g.sina[o];  // remap.py:34-39
+      const bool yaxis = c.line ? c.y : c.kind >= 2;  // contravariant component normal to the faces read
+      const T* G = g.gct + 4 * (long)o + (yaxis ? 2 : 0);
+      const T g0 = G[0], g1 = G[1], sn = g.sina[o];
+      if (c.line && want_h && c.q == 3) dz = (c.y ? g.dzph_y : g.dzph_x)[o];
+      T u = ua, v = va, h = ha;
+      if (vpull) {  // ext_vector / ext_scalar, cube.py:130-153
+        const T ull0 = c0[0] * ua + c0[1] * va, vll0 = c0[2] * ua + c0[3] * va;
+        const T ull1 = c1[0] * ub + c1[1] * vb, vll1 = c1[2] * ub + c1[3] * vb;
+        const T ull = p.w0 * ull0 + p.w1 * ull1;
+        const T vll = p.w0 * vll0 + p.w1 * vll1;
+        u = l2[0] * ull + l2[1] * vll;
+        v = l2[2] * ull + l2[3] * vll;
+        h = p.w0 * ha + p.w1 * hb;
+      }
+      const T ct = (g0 * u + g1 * v) * sn;  // remap.py:34-39
+      if (!c.line) {
         k.h[c.r * S::RJ + c.c] = h;
-        if (vert)
+        if (c.kind < 2)  // S/N halo rows belong to the vertical bar
           k.vb[c.r * TJ + (c.c - kHalo)] = ct;
         else
           k.hb[(c.r - kHalo) * S::RJ + c.c] = ct;
       } else {
-        T hn = pull_s(p, (const T*)io.h_out);
-        if (io.beta != T(0.0)) {
-          const T h = direct ? io.h[o] : pull_s(p, io.h);
-          hn = (T(1.0) - io.beta) * hn + io.beta * h;  // fb_scheme, barotr_pure.py:52-54
+        k.np[c.slot] = ct;
+        if (want_h) {
+          k.nh[c.slot] = h;
+          if (c.q == 3) k.ndz[c.slot / 6] = dz;
         }
-        k.h[c.r * S::RJ + c.c] = hn;
-        if (vert)
-          k.vb[c.r * TJ + (c.c - kHalo)] = v;
-        else
-          k.hb[(c.r - kHalo) * S::RJ + c.c] = u;
       }
-    } else {
-      const bool want_h = !UV && io.last;  // neighbour h for the mass-flux average
-      T u, v, h = T(0.0);
-      if (pull) {
-        pull_v(p, g, io.u, io.v, o, u, v);
-        if (want_h) h = pull_s(p, io.h);
-      } else {
-        u = io.u[o];
-        v = io.v[o];
-        if (want_h) h = io.h[o];
+    } else {  // region items only; the new h never has a stored halo
+      const bool blend = io.beta != T(0.0);
+      const T n0 = ((const T*)io.h_out)[p.s.x], n1 = ((const T*)io.h_out)[p.s.y];
+      T ba = T(0.0), bb = T(0.0);
+      if (blend) {
+        ba = io.h[sa];
+        bb = io.h[sb];
       }
-      const T dz = (want_h && c.q == 3) ? (c.y ? g.dzph_y[o] : g.dzph_x[o]) : T(0.0);
-      k.np[c.slot] = contra(g, o, u, v, c.y);
-      if (want_h) {
-        k.nh[c.slot] = h;
-        if (c.q == 3) k.ndz[c.slot / 6] = dz;
+      T u = ua, v = va, h = ba;
+      if (vpull) {
+        const T ull0 = c0[0] * ua + c0[1] * va, vll0 = c0[2] * ua + c0[3] * va;
+        const T ull1 = c1[0] * ub + c1[1] * vb, vll1 = c1[2] * ub + c1[3] * vb;
+        const T ull = p.w0 * ull0 + p.w1 * ull1;
+        const T vll = p.w0 * vll0 + p.w1 * vll1;
+        u = l2[0] * ull + l2[1] * vll;
+        v = l2[2] * ull + l2[3] * vll;
+        h = p.w0 * ba + p.w1 * bb;
       }
+      T hn = p.w0 * n0 + p.w1 * n1;
+      if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * h;  // fb_scheme, barotr_pure.py:52-54
+      k.h[c.r * S::RJ + c.c] = hn;
+      if (c.kind < 2)
+        k.vb[c.r * TJ + (c.c - kHalo)] = v;
+      else
+        k.hb[(c.r - kHalo) * S::RJ + c.c] = u;
     }
   }
 
