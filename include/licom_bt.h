@@ -112,7 +112,9 @@ typedef struct bt_state_out {
  * k2e_coef/loc_i/loc_j and the cube topology, allocates the stage scratch.
  * Replaces Schedule.configure/make_spmd_jit (schedule.py:209-243, spmd.py:38-75)
  * and Communication.configure (src/licom/kernel/communication.py:269-291).
- * The constant arrays must stay alive and unchanged while the plan exists. */
+ * The constant arrays must stay alive and unchanged while the plan exists;
+ * the 2x2 matrix arrays a_c2l, a_l2c and a_gct must start on a 16-byte
+ * boundary (BT_EINVAL otherwise). */
 int bt_plan_create(const bt_grid_desc* desc, bt_plan** out);
 
 /* Release a plan and everything it owns (no counterpart: JAX frees by refcount). */
@@ -192,7 +194,9 @@ int bt_conservation(int n, int dtype, const void* h, const void* u, const void* 
  * (held by every GPU that loads the library until exit): float64 rounds fit up
  * to N = 96, larger sizes return BT_EINVAL.  The first call on a device sets
  * up the array's address and must come before any stream capture.  Calls
- * share the array: calls whose GPU work overlaps race and must be serialised. */
+ * share the array: calls whose GPU work overlaps race and must be serialised.
+ * As for bt_plan_create, a_c2l, a_l2c and a_gct must start on a 16-byte
+ * boundary (BT_EINVAL otherwise). */
 int bt_round_noalloc(const bt_grid_desc* desc, const bt_state_in* in, const bt_state_out* out, int nbb,
                      double dtb, int rk, void* stream);
 

@@ -402,6 +402,7 @@ int bt_plan_create(const bt_grid_desc* d, bt_plan** out) {
                         d->rda, d->c_dy, d->d_dx};
   for (int k = 0; k < 17; ++k)
     if (!cs[k]) return fail(BT_EINVAL, "bt_plan_create: constant pointer " + std::to_string(k) + " is NULL");
+  if (!matrices_aligned(d)) return fail(BT_EINVAL, "bt_plan_create: a_c2l, a_l2c and a_gct must be 16-byte aligned");
   bt_plan* p = new bt_plan;
   p->n = d->n;
   p->m = d->n + 6;

@@ -30,6 +30,7 @@
 #include <string>
 
 #include "bt_launch.cuh"
+#include "bt_plan.cuh"
 #include "licom_bt.h"
 
 namespace bt {
@@ -299,6 +300,8 @@ extern "C" int bt_round_noalloc(const bt_grid_desc* desc, const bt_state_in* in,
                         desc->a_gct, desc->a_sina, desc->rda, desc->c_dy, desc->d_dx};
   for (const void* c : cs)
     if (!c) return set_error(BT_EINVAL, "bt_round_noalloc: NULL constant pointer");
+  if (!matrices_aligned(desc))
+    return set_error(BT_EINVAL, "bt_round_noalloc: a_c2l, a_l2c and a_gct must be 16-byte aligned");
   const void* ins[6] = {in->h0, in->h0p, in->ub, in->vb, in->ubp, in->vbp};
   for (const void* q : ins) {
     if (!q) return set_error(BT_EINVAL, "bt_round_noalloc: NULL input field");

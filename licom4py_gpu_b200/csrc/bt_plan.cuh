@@ -17,6 +17,13 @@
 
 using namespace bt;
 
+// The kernels read the 2x2 matrix arrays (a_c2l, a_l2c, a_gct: four values
+// per cell) with 16-byte copies and vector loads, so each must start on a
+// 16-byte boundary.
+inline bool matrices_aligned(const bt_grid_desc* d) {
+  return (((uintptr_t)d->a_c2l | (uintptr_t)d->a_l2c | (uintptr_t)d->a_gct) & 15) == 0;
+}
+
 struct bt_plan {
   int n = 0, m = 0, nh = 0, dtype = BT_F64, device = 0;
   TileCfg tile{8, 32};

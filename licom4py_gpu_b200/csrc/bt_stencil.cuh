@@ -322,6 +322,34 @@ __device__ __forceinline__ void cp_async_mat(T* dst, const T* src) {  // 4 conse
   }
 }
 
+// One 2x2 matrix (four consecutive values) or one row of it with vector
+// loads: bt_plan_create and bt_round_noalloc require the matrix arrays
+// (a_c2l, a_l2c, a_gct) to start on a 16-byte boundary.
+__device__ __forceinline__ void ld_quad(const float* p, float* q) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  q[0] = v.x;
+  q[1] = v.y;
+  q[2] = v.z;
+  q[3] = v.w;
+}
+__device__ __forceinline__ void ld_quad(const double* p, double* q) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  q[0] = a.x;
+  q[1] = a.y;
+  q[2] = b.x;
+  q[3] = b.y;
+}
+__device__ __forceinline__ void ld_pair(const float* p, float& a, float& b) {
+  const float2 v = *reinterpret_cast<const float2*>(p);
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void ld_pair(const double* p, double& a, double& b) {
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  a = v.x;
+  b = v.y;
+}
+
 // ---- halo gathers in two steps (descriptor, then sources) ------------------
 template <typename T>
 struct Pull {
@@ -515,12 +543,9 @@ struct Gather {
     const int sa = vpull ? p.s.x : o, sb = vpull ? p.s.y : o;
     const T ua = io.u[sa], va = io.v[sa], ub = io.u[sb], vb = io.v[sb];
     T c0[4], c1[4], l2[4];
-#pragma unroll
-    for (int z = 0; z < 4; ++z) {
-      c0[z] = g.c2l[4 * (long)sa + z];
-      c1[z] = g.c2l[4 * (long)sb + z];
-      l2[z] = g.l2c[4 * (long)o + z];
-    }
+    ld_quad(g.c2l + 4 * (long)sa, c0);
+    ld_quad(g.c2l + 4 * (long)sb, c1);
+    ld_quad(g.l2c + 4 * (long)o, l2);
     if (!UV) {
       const bool want_h = !c.line || io.last;  // region h, or the neighbour h of the mass-flux average
       T ha = T(0.0), hb = T(0.0), dz = T(0.0);
@@ -529,8 +554,9 @@ struct Gather {
         hb = io.h[sb];
       }
       const bool yaxis = c.line ? c.y : c.kind >= 2;  // contravariant component normal to the faces read
-      const T* G = g.gct + 4 * (long)o + (yaxis ? 2 : 0);
-      const T g0 = G[0], g1 = G[1], sn = g.sina[o];
+      T g0, g1;
+      ld_pair(g.gct + 4 * (long)o + (yaxis ? 2 : 0), g0, g1);
+      const T sn = g.sina[o];
       if (c.line && want_h && c.q == 3) dz = (c.y ? g.dzph_y : g.dzph_x)[o];
       T u = ua, v = va, h = ha;
       if (vpull) {  // ext_vector / ext_scalar, cube.py:130-153

@@ -45,12 +45,17 @@ def cuda_device(device=None) -> torch.device:
 
 
 def to_device(a, dtype: torch.dtype, device) -> torch.Tensor:
-    """Contiguous CUDA tensor of ``dtype`` (numpy arrays are copied once)."""
+    """Contiguous CUDA tensor of ``dtype`` starting on a 16-byte boundary (the
+    kernels read 2x2 matrices with 16-byte loads); numpy arrays and
+    misaligned views are copied once."""
     if isinstance(a, np.ndarray):
         a = torch.from_numpy(np.ascontiguousarray(a))
     if not isinstance(a, torch.Tensor):
         raise TypeError(f"expected a torch.Tensor or numpy.ndarray, got {type(a).__name__}")
-    return a.to(device=device, dtype=dtype).contiguous()
+    t = a.to(device=device, dtype=dtype).contiguous()
+    if t.data_ptr() % 16:
+        t = t.clone()
+    return t
 
 
 class BtPlan:

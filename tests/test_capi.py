@@ -44,6 +44,29 @@ def test_plan_create_rejects_bad_descriptor():
         _native.check(rc)
 
 
+def _fake_desc(misaligned):
+    """A descriptor with non-NULL placeholder pointers (never dereferenced: the
+    argument checks come first); ``misaligned`` names one pointer set 8 bytes
+    off a 16-byte boundary."""
+    desc = _native.GridDesc(48, _native.BT_F64)
+    for k, (name, _) in enumerate(_native.GridDesc._fields_[2:]):
+        setattr(desc, name, 0x10000 + 0x1000 * k + (8 if name == misaligned else 0))
+    return desc
+
+
+@pytest.mark.parametrize("name", ["a_c2l", "a_l2c", "a_gct"])
+def test_matrix_arrays_must_be_16_byte_aligned(name):
+    lib = _native.lib()
+    h = ctypes.c_void_p()
+    rc = lib.bt_plan_create(ctypes.byref(_fake_desc(name)), ctypes.byref(h))
+    assert rc == _native.BT_EINVAL and not h.value
+    assert b"16-byte aligned" in lib.bt_last_error()
+    sin, sout = _native.StateIn(), _native.StateOut()
+    rc = lib.bt_round_noalloc(ctypes.byref(_fake_desc(name)), ctypes.byref(sin), ctypes.byref(sout), 1, 10.0, 2, None)
+    assert rc == _native.BT_EINVAL
+    assert b"16-byte aligned" in lib.bt_last_error()
+
+
 def halo_tables(n, grid):
     c = make_consts(grid, 5000.0)
     m = n + 6

@@ -267,3 +267,31 @@ def test_persistent_barrier_timeout_is_reported_and_recoverable(grids):
     ref = BtPlan(consts).round(*ins, nbb=3, dtb=dtb)
     assert torch.equal(got["h0"], ref["h0"])
     p.close()
+
+
+def test_misaligned_constant_views_give_the_same_round(grids):
+    """Constant tensors that are views 8 bytes off a 16-byte boundary (the 2x2
+    matrices are read with 16-byte loads) are copied aligned by the plan."""
+    g = grids(24)
+    consts = make_consts(g, 5000.0)
+    s = harmonic_state(g, 5)
+    ins = [dev(s["h0"]), dev(s["h0"]), dev(s["ub"]), dev(s["vb"]), dev(s["ub"]), dev(s["vb"])]
+    dtb = cfl_dtb(g, 5000.0)
+    ref_plan = BtPlan(consts)
+    ref = ref_plan.round(*ins, nbb=3, dtb=dtb)
+    shifted = []
+    for c in consts:
+        t = torch.from_numpy(np.ascontiguousarray(c)).cuda()
+        buf = torch.empty(t.numel() + 1, dtype=t.dtype, device="cuda")
+        view = buf[1:].view(t.shape)
+        view.copy_(t)
+        shifted.append(view)
+    assert all(t.data_ptr() % 16 for t in shifted)
+    p = BtPlan(shifted)
+    assert all(t.data_ptr() % 16 == 0 for t in p.consts.values())
+    got = p.round(*ins, nbb=3, dtb=dtb)
+    torch.cuda.synchronize()
+    for k in ref:
+        assert torch.equal(ref[k], got[k]), k
+    p.close()
+    ref_plan.close()
