@@ -295,3 +295,45 @@ def test_misaligned_constant_views_give_the_same_round(grids):
         assert torch.equal(ref[k], got[k]), k
     p.close()
     ref_plan.close()
+
+
+# Tiles of 32 columns have full interior tiles (the whole stencil region inside
+# the face, compiled without the edge logic) only from C96 on; these cases run
+# every full-tile instantiation next to edge tiles.
+@pytest.mark.parametrize("tile", [(7, 32), (8, 32), (15, 32), (16, 32), (16, 16)])
+def test_full_tile_shapes_bitwise_identical_c96(tile, grids):
+    g = grids(96)
+    consts = make_consts(g, 5000.0)
+    s = harmonic_state(g, 12)
+    ins = [dev(s["h0"]), dev(s["h0"]), dev(s["ub"]), dev(s["vb"]), dev(s["ub"]), dev(s["vb"])]
+    dtb = cfl_dtb(g, 5000.0)
+    ref_plan, plan = BtPlan(consts, tile=(8, 16)), BtPlan(consts, tile=tile)
+    for rk in (2, 3):
+        ref = ref_plan.round(*ins, nbb=3, dtb=dtb, rk=rk)
+        got = plan.round(*ins, nbb=3, dtb=dtb, rk=rk)
+        for k in ref:
+            assert torch.equal(ref[k], got[k]), (tile, rk, k)
+    ref_plan.close()
+    plan.close()
+
+
+@pytest.mark.parametrize("tile", [(7, 32), (8, 32), (15, 32), (16, 32), (8, 16), (16, 16)])
+def test_float32_full_tiles_c96(tile, grids):
+    """Float32 rounds at C96 (full interior tiles of every shape) against the float64 path: 1e-5
+    relative L2 on h, u, v after 100 substeps."""
+    g = grids(96)
+    consts = make_consts(g, 5000.0)
+    s = harmonic_state(g, 13)
+    dtb = cfl_dtb(g, 5000.0)
+    keys = ("h0", "h0", "ub", "vb", "ub", "vb")
+    p64 = BtPlan(consts, tile=(8, 16))
+    want = p64.round(*[dev(s[k]) for k in keys], nbb=100, dtb=dtb, diag=False)
+    p32 = BtPlan(consts, dtype=torch.float32, tile=tile)
+    got = p32.round(*[dev(s[k], torch.float32) for k in keys], nbb=100, dtb=dtb, diag=False)
+    for key in ("h0", "ub", "vb"):
+        a = got[key][:, 3:-3, 3:-3].double()
+        b = want[key][:, 3:-3, 3:-3]
+        l2 = ((a - b).norm() / b.norm()).item()
+        assert l2 <= 1e-5, f"{tile} {key}: relative L2 error {l2:.2e}"
+    p64.close()
+    p32.close()
