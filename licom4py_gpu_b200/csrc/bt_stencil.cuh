@@ -232,7 +232,6 @@ struct TileShape {
   static constexpr int KV = (RI + NS - 1) / NS;     // row iterations over the vertical bar
   static constexpr int KX = (TI + 1 + NS - 1) / NS; // over x-face rows
   static constexpr int KC = (TI + NS - 1) / NS;     // over tile rows
-  static constexpr int MI = 2;                      // gather items per thread handled in the two-sweep path
   // phase H (words): s_h [RI][RJ], s_uc [VB], s_vc [TI][RJ], s_g [NP][4], s_sn [NP],
   // s_dzx/s_cdy [FX], s_dzy/s_ddx [FY], s_rda [C], neighbour lines; s_P [FX] and
   // s_Q [FY] alias s_g (dead once the region is staged)
@@ -506,27 +505,25 @@ struct Gather {
   // phase H gathers the region halo and the neighbour edge lines (9 items per
   // edge position); phase UV only the region halo (3 per position)
   static constexpr int kPerPos = UV ? 3 : 9;
-  Pull<T> pd[S::MI];
-  bool pl[S::MI];
+  Pull<T> pd;  // descriptor of the thread's first item
+  bool pl;
 
   __device__ __forceinline__ static bool needs_pull(const StageIO<T>& io, const ItemCell& c, int m) {
     return !is_interior(c.i, c.j, m) && (!io.stored_halo || (UV && !c.line));
   }
 
-  // sweep 1: descriptors of the items' halo gathers (constants, may precede the grid dependency)
+  // sweep 1: the descriptor of the thread's first item (constants, may
+  // precede the grid dependency)
   __device__ __forceinline__ void descriptors(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
                                               const EdgeCnt& cnt, int P) {
-    const int nitems = kPerPos * P;
-#pragma unroll
-    for (int k = 0; k < S::MI; ++k) {
-      const int t = threadIdx.x + k * kTileThreads;
-      pl[k] = false;
-      if (t < nitems) {
-        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
-        if (needs_pull(io, c, g.m)) {
-          pd[k] = pull_desc(g, c.f, c.i, c.j);
-          pl[k] = true;
-        }
+    pl = false;
+    pd.s = make_int2(0, 0);
+    pd.w0 = pd.w1 = T(0.0);
+    if ((int)threadIdx.x < kPerPos * P) {
+      const ItemCell c = decode_item(b, cnt, P, threadIdx.x, g.m, g.n, S::EW);
+      if (needs_pull(io, c, g.m)) {
+        pd = pull_desc(g, c.f, c.i, c.j);
+        pl = true;
       }
     }
   }
@@ -610,24 +607,23 @@ struct Gather {
     }
   }
 
-  // sweep 2: sources (state, after the grid dependency) and the items' values
+  // sweep 2: sources (state, after the grid dependency) and the items'
+  // values.  One rolled loop, so the item code exists once in the kernel (the
+  // edge path is cold code: at small sizes each CTA runs it once and waits on
+  // instruction fetch); items past the first of a thread (tiles with more than
+  // kTileThreads items) load their descriptor here.
   __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
                                           const EdgeCnt& cnt, int P, const GatherSink<T>& k) {
     const int nitems = kPerPos * P;
-#pragma unroll
-    for (int q = 0; q < S::MI; ++q) {
-      const int t = threadIdx.x + q * kTileThreads;
-      if (t < nitems) {
-        const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
-        one(g, io, c, pd[q], pl[q], k);
-      }
-    }
-    // items beyond MI per thread (only tiles spanning several face edges of tiny faces)
-    for (int t = threadIdx.x + S::MI * kTileThreads; t < nitems; t += kTileThreads) {
+#pragma unroll 1
+    for (int t = threadIdx.x; t < nitems; t += kTileThreads) {
       const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
-      const bool pull = needs_pull(io, c, g.m);
-      Pull<T> p;
-      if (pull) p = pull_desc(g, c.f, c.i, c.j);
+      bool pull = pl;
+      Pull<T> p = pd;
+      if (t >= kTileThreads) {
+        pull = needs_pull(io, c, g.m);
+        if (pull) p = pull_desc(g, c.f, c.i, c.j);
+      }
       one(g, io, c, p, pull, k);
     }
   }
