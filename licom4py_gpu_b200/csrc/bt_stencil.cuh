@@ -836,16 +836,11 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
 #pragma unroll
   for (int k = 0; k < S::KV; ++k) {
     const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-    if (q < nj && r < ni + 6 && (FULL || ec.row_staged(i, m))) {
-      if (FULL || (i >= kHalo && i < m - kHalo)) {
-        const int o = ov + r * m;
-        hv[k] = io.h[o];
-        uv[k] = io.u[o];
-        vv[k] = io.v[o];
-      } else {
-        hv[k] = fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
-        fetch_v(io.u, io.v, g, f, i, b.j0 + q, io.stored_halo, uv[k], vv[k]);
-      }
+    if (q < nj && r < ni + 6 && (FULL || (i >= kHalo && i < m - kHalo))) {  // halo rows: see below
+      const int o = ov + r * m;
+      hv[k] = io.h[o];
+      uv[k] = io.u[o];
+      vv[k] = io.v[o];
     }
   }
   const int t6 = threadIdx.x;
@@ -875,13 +870,31 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
 #pragma unroll
   for (int k = 0; k < S::KV; ++k) {
     const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-    if (q < nj && r < ni + 6 && (FULL || ec.row_staged(i, m))) {
+    if (q < nj && r < ni + 6 && (FULL || (i >= kHalo && i < m - kHalo))) {
       const int p = r * TJ + q;
       const T* G = L.s_g + 4 * p;
       const T sn = L.s_sn[p], u = uv[k], v = vv[k];
       L.s_h[r * RJ + q + kHalo] = hv[k];
       L.s_uc[p] = (G[0] * u + G[1] * v) * sn;
       if (r >= kHalo && r < ni + kHalo) L.s_vc[(r - kHalo) * RJ + q + kHalo] = (G[2] * u + G[3] * v) * sn;
+    }
+  }
+  if (!FULL) {
+    // halo rows of the region that no gather item covers (EdgeCover), fetched
+    // point by point; a rolled loop keeps this rarely run code small
+#pragma unroll 1
+    for (int k = 0; k < S::KV; ++k) {
+      const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
+      if (q < nj && r < ni + 6 && ec.row_staged(i, m) && !(i >= kHalo && i < m - kHalo)) {
+        T u, v;
+        const T h = fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
+        fetch_v(io.u, io.v, g, f, i, b.j0 + q, io.stored_halo, u, v);
+        const int p = r * TJ + q;
+        const T* G = L.s_g + 4 * p;
+        const T sn = L.s_sn[p];
+        L.s_h[r * RJ + q + kHalo] = h;
+        L.s_uc[p] = (G[0] * u + G[1] * v) * sn;
+      }
     }
   }
   if (side_pt) {
@@ -1082,22 +1095,30 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
 #pragma unroll
   for (int k = 0; k < S::KV; ++k) {
     const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
-    if (q < nj && r < ni + 6 && (FULL || ec.row_staged(i, m))) {
+    if (q < nj && r < ni + 6 && (FULL || (i >= kHalo && i < m - kHalo))) {  // halo rows: see below
       const bool row = r >= kHalo && r < ni + kHalo;
       const int e = r * RJ + q + kHalo;
-      if (FULL || (i >= kHalo && i < m - kHalo)) {
-        const int o = ov + r * m;
-        cp_async_t(L.s_hn + e, hn_src + o);
-        if (blend) cp_async_t(L.s_hb + e, io.h + o);
-        cp_async_t(L.s_v + r * TJ + q, io.v + o);
-        if (row) cp_async_t(L.s_u + (r - kHalo) * RJ + q + kHalo, io.u + o);
-      } else {  // the new h never has a stored halo
+      const int o = ov + r * m;
+      cp_async_t(L.s_hn + e, hn_src + o);
+      if (blend) cp_async_t(L.s_hb + e, io.h + o);
+      cp_async_t(L.s_v + r * TJ + q, io.v + o);
+      if (row) cp_async_t(L.s_u + (r - kHalo) * RJ + q + kHalo, io.u + o);
+    }
+  }
+  if (!FULL) {
+    // halo rows of the region that no gather item covers (EdgeCover), fetched
+    // point by point and stored blended (the new h never has a stored halo)
+#pragma unroll 1
+    for (int k = 0; k < S::KV; ++k) {
+      const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
+      if (q < nj && r < ni + 6 && ec.row_staged(i, m) && !(i >= kHalo && i < m - kHalo)) {
+        const int e = r * RJ + q + kHalo;
         T hn = fetch_s(hn_src, g, f, i, b.j0 + q, 0), u, v;
         fetch_v(io.u, io.v, g, f, i, b.j0 + q, io.stored_halo, u, v);
         if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
         L.s_hn[e] = hn;
         L.s_v[r * TJ + q] = v;
-        if (row) L.s_u[(r - kHalo) * RJ + q + kHalo] = u;
+        if (r >= kHalo && r < ni + kHalo) L.s_u[(r - kHalo) * RJ + q + kHalo] = u;
       }
     }
   }
