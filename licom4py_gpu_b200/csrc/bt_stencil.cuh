@@ -364,24 +364,6 @@ __device__ __forceinline__ Pull<T> pull_desc(const Geo<T>& g, int f, int i, int 
   p.w1 = g.hw[2 * k + 1];
   return p;
 }
-template <typename T>
-__device__ __forceinline__ T pull_s(const Pull<T>& p, const T* F) {
-  return p.w0 * F[p.s.x] + p.w1 * F[p.s.y];
-}
-template <typename T>
-__device__ __forceinline__ void pull_v(const Pull<T>& p, const Geo<T>& g, const T* U, const T* V, long o,
-                                       T& u, T& v) {
-  const T* C0 = g.c2l + 4 * (long)p.s.x;
-  const T* C1 = g.c2l + 4 * (long)p.s.y;
-  const T u0 = U[p.s.x], v0 = V[p.s.x], u1 = U[p.s.y], v1 = V[p.s.y];
-  const T ull0 = C0[0] * u0 + C0[1] * v0, vll0 = C0[2] * u0 + C0[3] * v0;
-  const T ull1 = C1[0] * u1 + C1[1] * v1, vll1 = C1[2] * u1 + C1[3] * v1;
-  const T ull = p.w0 * ull0 + p.w1 * ull1;
-  const T vll = p.w0 * vll0 + p.w1 * vll1;
-  const T* L = g.l2c + 4 * o;
-  u = L[0] * ull + L[1] * vll;
-  v = L[2] * ull + L[3] * vll;
-}
 
 // ---- the tile's face-edge positions ----------------------------------------
 // Item q of a tile's edge list: kind 0/1 = x faces of side S/N (position along
