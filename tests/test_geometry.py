@@ -79,3 +79,34 @@ def test_make_consts_order(grids):
     assert len(c) == 17
     assert c[6].dtype == np.int32 and c[7].dtype == np.int32
     assert c[0][0, 0, 0] == 5600.0
+
+
+def _halo_fill_error(n, grids):
+    """Max error of the duogrid halo fill (the host gather table: two interior sources, two
+    weights per halo cell) of a smooth analytic field against the field at the halo points, over
+    the halo cells beside the face edges.  The 3 x 3 corner blocks are excluded: the reference
+    fills them by copying the adjacent band cell, not by interpolation."""
+    from test_capi import halo_cells, halo_tables
+    g = grids(n)
+    src, w, _, _ = halo_tables(n, g)
+    lon, lat = g["a_pt"][..., 0], g["a_pt"][..., 1]
+    field = np.cos(lat) * np.cos(lon - 0.3) + 0.5 * np.sin(lat) ** 2  # smooth on the sphere
+    flat = field.reshape(-1)
+    m = n + 6
+    err = 0.0
+    for f in range(6):
+        for k, (i, j) in enumerate(halo_cells(m)):
+            if (i < H or i >= m - H) and (j < H or j >= m - H):
+                continue
+            a, b = src[f, k]
+            got = w[f, k, 0] * flat[a] + w[f, k, 1] * flat[b]
+            err = max(err, abs(got - field[f, i, j]))
+    return err
+
+
+def test_halo_fill_of_a_smooth_field_is_second_order(grids):
+    """The halo fill (update_domain + the linear cube_rmp remap) interpolates linearly: its error on a
+    smooth field of unit size is small and falls about 4x when the resolution doubles."""
+    e24, e48 = _halo_fill_error(24, grids), _halo_fill_error(48, grids)
+    assert e48 < 1e-3
+    assert e24 / e48 > 3.5, (e24, e48)
