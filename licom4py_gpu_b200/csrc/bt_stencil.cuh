@@ -257,7 +257,48 @@ struct TileBox {
   int f, i0, j0, ni, nj;
 };
 
-__device__ __forceinline__ TileBox tile_box(const Tiling& t, int n, int tile) {
+// Work order of the tiles: the tiles on the ring of each face's tile grid
+// (those touching a face edge: halo gathers and edge averages make them the
+// slowest) come first, the interior tiles after them, so that the long tiles
+// start in the first wave instead of finishing a launch alone (largest work
+// first).  Item b < 6 R (R = ring tiles of one face) is ring tile b % R of face
+// b / R; the rest are the interior tiles face by face.  Returns the tile's
+// face-major, row-major index.
+__device__ __forceinline__ int edge_first_tile(const Tiling& t, int b) {
+  const int nti = t.nti, ntj = t.ntj;
+  if (nti < 3 || ntj < 3) return b;  // every tile touches a face edge
+  const int R = 2 * ntj + 2 * (nti - 2);
+  int f, ti, tj;
+  if (b < 6 * R) {
+    f = b / R;
+    int r = b - f * R;
+    if (r < ntj) {
+      ti = 0;
+      tj = r;
+    } else if ((r -= ntj) < ntj) {
+      ti = nti - 1;
+      tj = r;
+    } else if ((r -= ntj) < nti - 2) {
+      ti = 1 + r;
+      tj = 0;
+    } else {
+      ti = 1 + r - (nti - 2);
+      tj = ntj - 1;
+    }
+  } else {
+    const int I = (nti - 2) * (ntj - 2), k = b - 6 * R;
+    f = k / I;
+    const int rr = k - f * I;
+    ti = 1 + rr / (ntj - 2);
+    tj = 1 + rr % (ntj - 2);
+  }
+  return (f * nti + ti) * ntj + tj;
+}
+
+// The tile that work item ``item`` (a CTA of a phase launch, or a step of a
+// persistent CTA's tile loop) computes, in edge_first_tile order.
+__device__ __forceinline__ TileBox tile_box(const Tiling& t, int n, int item) {
+  const int tile = edge_first_tile(t, item);
   TileBox b;
   const int per_face = t.nti * t.ntj;
   b.f = tile / per_face;
