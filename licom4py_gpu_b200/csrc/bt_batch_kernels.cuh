@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kTileThreads, kBatchPhaseBlocks) k_batch_phase
   const int k = s_k;
   ctx_load(ctx, a, k, step, st);
   const Geo<T>& g = ctx.g;
-  const TileBox b = tile_box(make_tiling_dev(TI, TJ, g.n), g.n, tile - __ldg(a.off.tile + k));
+  const TileBox b = tile_box_at(make_tiling_dev(TI, TJ, g.n), g.n, tile - __ldg(a.off.tile + k));
   T* sm = reinterpret_cast<T*>(smraw);
   if (!UV)
     tile_h<T, TI, TJ>(g, ctx.io, b, sm);
