@@ -264,7 +264,7 @@ namespace {
 template <typename T, int TI, int TJ, bool UV>
 size_t batch_tile_smem() {
   using S = TileShape<TI, TJ>;
-  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH);
+  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH) + sizeof(int) * kItemWords;
 }
 
 template <typename T, int TI, int TJ>

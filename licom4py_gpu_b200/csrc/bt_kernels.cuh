@@ -136,7 +136,7 @@ namespace {
 template <typename T, int TI, int TJ, bool UV>
 size_t tile_smem() {
   using S = TileShape<TI, TJ>;
-  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH);
+  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH) + sizeof(int) * kItemWords;
 }
 
 // The persistent kernel runs both phases in one allocation: the larger of the two.

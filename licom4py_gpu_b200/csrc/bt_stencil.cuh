@@ -469,11 +469,36 @@ __device__ __forceinline__ EdgeItem edge_item(const TileBox& b, const EdgeCnt& c
 // two L2 round trips instead of one chain per point.
 struct ItemCell {
   int f, i, j;      // cell whose value the item needs
+  int o;            // its offset within the member, cell32(f, i, j, m)
   int kind;         // edge kind 0..3 (S, N, W, E)
   int r, c;         // region row / column (region items)
   int slot;         // line item: edge slot * 6 + q
   int line, y, q;   // line item: 1, normal axis (1 = y), point index
 };
+
+// Shared-memory words (ints) past a phase's layout where each thread keeps
+// its first gather item, decoded in the prologue: the offset o at [t] and the
+// other fields the item needs at [kTileThreads + t], packed as
+// r | c << 6 | slot << 12 | line << 22 | kind << 23 | y << 25 | (q == 3) << 26.
+// Only the writing thread reads them back (after the grid dependency), so the
+// decode's cold code stays off the critical path without holding registers.
+constexpr int kItemWords = 2 * kTileThreads;
+__device__ __forceinline__ int pack_item(const ItemCell& c) {
+  return c.r | (c.c << 6) | (c.slot << 12) | (c.line << 22) | (c.kind << 23) | (c.y << 25) | ((c.q == 3) << 26);
+}
+__device__ __forceinline__ ItemCell unpack_item(int o, int pk) {
+  ItemCell c;
+  c.f = c.i = c.j = 0;  // not needed past the descriptor sweep
+  c.o = o;
+  c.r = pk & 63;
+  c.c = (pk >> 6) & 63;
+  c.slot = (pk >> 12) & 1023;
+  c.line = (pk >> 22) & 1;
+  c.kind = (pk >> 23) & 3;
+  c.y = (pk >> 25) & 1;
+  c.q = ((pk >> 26) & 1) ? 3 : 0;
+  return c;
+}
 
 __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const EdgeCnt& cnt, int P, int t, int m, int n,
                                                 int EW) {
@@ -491,6 +516,7 @@ __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const EdgeCnt&
     c.f = b.f;
     c.i = b.i0 - kHalo + r;
     c.j = b.j0 - kHalo + cc;
+    c.o = cell32(c.f, c.i, c.j, m);
     c.kind = e.kind;
     c.r = r;
     c.c = cc;
@@ -507,6 +533,7 @@ __device__ __forceinline__ ItemCell decode_item(const TileBox& b, const EdgeCnt&
     const int kk = route_rev(r) ? n - 1 - e.k : e.k;
     c.f = route_nb(r);
     edge_point(ns, kk, q, m, c.i, c.j);
+    c.o = cell32(c.f, c.i, c.j, m);
     c.kind = e.kind;
     c.r = 0;
     c.c = 0;
@@ -545,12 +572,14 @@ struct Gather {
   // sweep 1: the descriptor of the thread's first item (constants, may
   // precede the grid dependency)
   __device__ __forceinline__ void descriptors(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
-                                              const EdgeCnt& cnt, int P) {
+                                              const EdgeCnt& cnt, int P, int* s_items) {
     pl = false;
     pd.s = make_int2(0, 0);
     pd.w0 = pd.w1 = T(0.0);
     if ((int)threadIdx.x < kPerPos * P) {
       const ItemCell c = decode_item(b, cnt, P, threadIdx.x, g.m, g.n, S::EW);
+      s_items[threadIdx.x] = c.o;
+      s_items[kTileThreads + threadIdx.x] = pack_item(c);
       if (needs_pull(io, c, g.m)) {
         pd = pull_desc(g, c.f, c.i, c.j);
         pl = true;
@@ -565,7 +594,7 @@ struct Gather {
   // read stays exact), and all loads precede the item's shared-memory stores.
   __device__ __forceinline__ void one(const Geo<T>& g, const StageIO<T>& io, const ItemCell& c, const Pull<T>& p,
                                       bool pull, const GatherSink<T>& k) {
-    const int o = cell32(c.f, c.i, c.j, g.m);
+    const int o = c.o;
     const bool vpull = UV ? !io.stored_halo : pull;  // velocity interpolated (else read directly)
     const int sa = vpull ? p.s.x : o, sb = vpull ? p.s.y : o;
     const T ua = io.u[sa], va = io.v[sa], ub = io.u[sb], vb = io.v[sb];
@@ -643,14 +672,17 @@ struct Gather {
   // instruction fetch); items past the first of a thread (tiles with more than
   // kTileThreads items) load their descriptor here.
   __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
-                                          const EdgeCnt& cnt, int P, const GatherSink<T>& k) {
+                                          const EdgeCnt& cnt, int P, const GatherSink<T>& k, const int* s_items) {
     const int nitems = kPerPos * P;
 #pragma unroll 1
     for (int t = threadIdx.x; t < nitems; t += kTileThreads) {
-      const ItemCell c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
       bool pull = pl;
       Pull<T> p = pd;
-      if (t >= kTileThreads) {
+      ItemCell c;
+      if (t < kTileThreads) {
+        c = unpack_item(s_items[t], s_items[kTileThreads + t]);
+      } else {
+        c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
         pull = needs_pull(io, c, g.m);
         if (pull) p = pull_desc(g, c.f, c.i, c.j);
       }
@@ -804,7 +836,7 @@ __device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& 
     P = 0;
   } else {
     P = edge_count(b, m, g.route, cnt);
-    if (P > 0) gat.descriptors(g, io, b, cnt, P);
+    if (P > 0) gat.descriptors(g, io, b, cnt, P, reinterpret_cast<int*>(sm + S::kWordsH));
   }
 }
 
@@ -892,7 +924,9 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
     const int a = sl + k * S::NS;
     if (q < nj && a < ni) hpc[k] = io.hp[ov + (a + kHalo) * m];
   }
-  if (!FULL && P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_h, L.s_uc, L.s_vc, L.s_np, L.s_nh, L.s_ndz});
+  if (!FULL && P > 0)
+    gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_h, L.s_uc, L.s_vc, L.s_np, L.s_nh, L.s_ndz},
+                reinterpret_cast<const int*>(sm + S::kWordsH));
   cp_async_wait_all();
   __syncthreads();
 
@@ -1065,7 +1099,7 @@ __device__ __forceinline__ void tile_uv_pro_t(const Geo<T>& g, const StageIO<T>&
     P = 0;
   } else {
     P = edge_count(b, m, g.route, cnt);
-    if (P > 0) gat.descriptors(g, io, b, cnt, P);
+    if (P > 0) gat.descriptors(g, io, b, cnt, P, reinterpret_cast<int*>(sm + S::kWordsUV));
   }
 }
 
@@ -1179,7 +1213,9 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
       vpc[k] = io.vp[ov + (a + kHalo) * m];
     }
   }
-  if (!FULL && P > 0) gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr});
+  if (!FULL && P > 0)
+    gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr},
+                reinterpret_cast<const int*>(sm + S::kWordsUV));
   cp_async_wait_all();
   __syncthreads();
   if (blend) {  // fb_scheme, barotr_pure.py:52-54, on the points staged by cp.async
