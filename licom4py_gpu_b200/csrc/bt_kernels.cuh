@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kThreads, PhaseBlocks<T>::value) k_phase_h(Geo
 }
 
 template <typename T, int TI, int TJ>
-__global__ void __launch_bounds__(kThreads, PhaseBlocks<T>::value) k_phase_uv(Geo<T> g, StageIO<T> io, Tiling t) {
+__global__ void __launch_bounds__(kThreads, PhaseBlocksUV<T>::value) k_phase_uv(Geo<T> g, StageIO<T> io, Tiling t) {
   extern __shared__ __align__(16) unsigned char smraw[];
   release_dependents();
   const TileBox b = tile_box(t, g.n, blockIdx.x);

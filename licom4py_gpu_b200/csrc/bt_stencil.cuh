@@ -212,6 +212,12 @@ template <typename T>
 struct PhaseBlocks {
   static constexpr int value = sizeof(T) == 8 ? 3 : 4;
 };
+// Phase UV runs 3 CTAs per SM in both precisions: at 4 its shared-memory
+// traffic throttles (MIO) and the best tile shape per size measured faster at 3.
+template <typename T>
+struct PhaseBlocksUV {
+  static constexpr int value = 3;
+};
 
 constexpr int up4(int x) { return (x + 3) & ~3; }  // shared-memory offsets in words, 16-byte aligned
 
