@@ -43,15 +43,20 @@ extern "C" {
 #define BT_MODE_STREAM 0      /* kernels launched in stream order */
 #define BT_MODE_GRAPH 1       /* the round is captured once as a CUDA graph and replayed */
 #define BT_MODE_PERSISTENT 2  /* one cooperative launch with grid barriers per round */
+#define BT_MODE_RESIDENT 3    /* one cooperative launch per round, one CTA per tile holding its constants
+                                 and face cache on chip, neighbour tiles synchronised by progress flags;
+                                 grids whose tiles all fit on the GPU at once (else BT_ENOTSUP) */
 
 /* Plan options (bt_plan_set_option) */
 #define BT_OPT_MAX_CTAS 1    /* persistent mode: cap on the cooperative grid (0 = occupancy limit) */
-#define BT_OPT_SPIN_LIMIT 2  /* persistent mode: polls a grid-barrier wait may take before it gives up */
-#define BT_OPT_KERNEL_TIMING 3  /* 1 = bracket the round kernel (persistent mode) or each phase kernel
-                                   (stream mode) with CUDA events on its stream; setting it resets the record */
+#define BT_OPT_SPIN_LIMIT 2  /* persistent / resident mode: polls a grid-barrier or neighbour wait may
+                                take before it gives up */
+#define BT_OPT_KERNEL_TIMING 3  /* 1 = bracket the round kernel (persistent / resident mode) or each phase
+                                   kernel (stream mode) with CUDA events on its stream; setting it resets
+                                   the record */
 
 /* Kernel kinds of bt_plan_kernel_time */
-#define BT_KERNEL_ROUND 0     /* the persistent round kernel */
+#define BT_KERNEL_ROUND 0     /* the persistent or resident round kernel */
 #define BT_KERNEL_PHASE_H 1   /* the h-update tile kernel of a stage */
 #define BT_KERNEL_PHASE_UV 2  /* the momentum-update tile kernel of a stage */
 
@@ -191,12 +196,19 @@ int bt_conservation(int n, int dtype, const void* h, const void* u, const void* 
  * Same arguments and results as bt_round, but no plan: desc is passed directly
  * and the halo tables are rebuilt on the device each call, stream-ordered.
  * All scratch lives in one 6 MiB array the library declares statically
- * (held by every GPU that loads the library until exit): float64 rounds fit up
- * to N = 96, larger sizes return BT_EINVAL.  The first call on a device sets
- * up the array's address and must come before any stream capture.  Calls
- * share the array: calls whose GPU work overlaps race and must be serialised.
- * As for bt_plan_create, a_c2l, a_l2c and a_gct must start on a 16-byte
- * boundary (BT_EINVAL otherwise). */
+ * (held by every GPU that loads the library until exit).  Largest sizes:
+ * float64 N <= 116 (rk 2) / 99 (rk 3), float32 N <= 165 (rk 2) / 142 (rk 3);
+ * larger sizes return BT_EINVAL.  The first call on a device sets up the
+ * array's address and must come before any stream capture.  The first call
+ * with a given set of constant pointers on a device checks the tables as
+ * bt_plan_create does (k2e locations inside the band: BT_EINVAL; inner/outer
+ * the exact masks: BT_ENOTSUP) and synchronises the stream to read the
+ * result; later calls with the same pointers skip the check, so the tables
+ * must not change meanwhile.  Calls share the array: calls whose GPU work
+ * overlaps race and must be serialised.  The round runs the 8 x 16 tile shape
+ * whatever bt_plan_set_tile a plan would use (float64 results are the same for
+ * every shape).  As for bt_plan_create, a_c2l, a_l2c and a_gct must start on a
+ * 16-byte boundary (BT_EINVAL otherwise). */
 int bt_round_noalloc(const bt_grid_desc* desc, const bt_state_in* in, const bt_state_out* out, int nbb,
                      double dtb, int rk, void* stream);
 

@@ -1,8 +1,9 @@
 """Autotuner for the round execution mode and tile shape.
 
 For one resolution N and dtype it times short rounds of every candidate
-(mode in {persistent, graph}) x (tile shape) on the current GPU and keeps the
-fastest.  Results are cached per (GPU name, N, dtype) in a JSON file
+(mode in {resident, persistent, graph}) x (tile shape) on the current GPU and
+keeps the fastest; resident candidates whose tiles do not all fit on the GPU
+at once (or whose tile shape has no resident kernel) are skipped.  Results are cached per (GPU name, N, dtype) in a JSON file
 (``$LICOM_BT_TUNE_CACHE``, default ``~/.cache/licom4py_gpu_b200/tune.json``).
 Without constants to time with, a static heuristic is returned.
 """
@@ -16,7 +17,7 @@ from typing import Dict, Optional, Sequence
 import torch
 
 TILES = ((7, 32), (8, 32), (15, 32), (16, 32), (8, 16), (16, 16))
-MODES = ("persistent", "graph")
+MODES = ("resident", "persistent", "graph")
 
 
 def _cache_path() -> str:
@@ -47,11 +48,12 @@ def _store(key: str, cfg: dict) -> None:
 
 
 def heuristic(n: int) -> dict:
-    """Static choice: small grids are barrier/launch bound -> persistent; large ones graph."""
-    if n <= 64:
-        return {"mode": "persistent", "tile": [8, 16], "source": "heuristic"}
+    """Static choice: grids whose 8 x 16 tiles all fit on the GPU at once run
+    tile-resident; larger ones as CUDA graphs."""
+    if n <= 96:
+        return {"mode": "resident", "tile": [8, 16], "source": "heuristic"}
     if n <= 192:
-        return {"mode": "persistent", "tile": [8, 32], "source": "heuristic"}
+        return {"mode": "graph", "tile": [8, 32], "source": "heuristic"}
     return {"mode": "graph", "tile": [16, 32], "source": "heuristic"}
 
 
@@ -79,7 +81,10 @@ def tune(n: int, dtype: torch.dtype, consts: Sequence, device=None, nbb: int = 4
             p = BtPlan(consts, dtype=dtype, device=dev, tile=tile, mode=mode)
             out = None
             try:
-                out = p.round(*ins, nbb=nbb, dtb=dtb, diag=False)
+                try:
+                    out = p.round(*ins, nbb=nbb, dtb=dtb, diag=False)
+                except NotImplementedError:  # resident mode: shape without a kernel, or too many tiles
+                    continue
                 torch.cuda.synchronize(dev)
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record()

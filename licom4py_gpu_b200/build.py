@@ -34,9 +34,10 @@ CXX = os.environ.get("CXX", shutil.which("g++") or "g++")
 CUDA_SOURCES = [("bt_kernels_f64.cu", ["-fmad=false"]), ("bt_kernels_f32.cu", ["-fmad=true"]),
                 ("bt_capi.cu", ["-fmad=false"]), ("bt_reduce.cu", ["-fmad=false"]),
                 ("bt_noalloc.cu", ["-fmad=false"]), ("bt_batch_f64.cu", ["-fmad=false"]),
-                ("bt_batch_f32.cu", ["-fmad=true"]), ("bt_batch_capi.cu", ["-fmad=false"])]
+                ("bt_batch_f32.cu", ["-fmad=true"]), ("bt_batch_capi.cu", ["-fmad=false"]),
+                ("bt_resident_f64.cu", ["-fmad=false"]), ("bt_resident_f32.cu", ["-fmad=true"])]
 CUDA_HEADERS = ["bt_common.cuh", "bt_stencil.cuh", "bt_launch.cuh", "bt_kernels.cuh", "bt_plan.cuh",
-                "bt_batch.cuh", "bt_batch_kernels.cuh"]
+                "bt_batch.cuh", "bt_batch_kernels.cuh", "bt_resident.cuh"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -173,6 +174,7 @@ int build_tables(bt_plan* p, const bt_grid_desc* d) {
   std::vector<T> w((size_t)6 * nh * 2);
   const int rc = build_halo_host<T>(p->n, coef.data(), li.data(), lj.data(), src.data(), w.data(), p->route);
   if (rc != BT_OK) return rc;
+  p->h_src = src;
   BT_CUDA(cudaMalloc(&p->d_hsrc, src.size() * sizeof(int2)), "alloc halo table");
   BT_CUDA(cudaMalloc(&p->d_hw, w.size() * sizeof(T)), "alloc halo weights");
   BT_CUDA(cudaMemcpy(p->d_hsrc, src.data(), src.size() * sizeof(int2), cudaMemcpyHostToDevice), "upload table");
@@ -281,10 +283,16 @@ cudaError_t enqueue_stage(const bt_plan* p, const bt_state_in& in, const bt_stat
   return launch_fill_halo<T>(g, X[0], X[1], X[2], s);
 }
 
-// Persistent mode: one cooperative launch runs every phase of every substep.
+// Substeps per cooperative launch of the persistent and resident modes: a
+// round is split into launches of at most this many substeps, so the grid
+// barrier's 31-bit arrival count (2 x stages x substeps x CTAs) and the
+// resident progress flags (2 x stages x substeps) stay far from overflow.
+constexpr int kSubstepsPerLaunch = 1 << 16;
+
+// The launch arguments of a whole round (persistent and resident modes).
 template <typename T>
-cudaError_t enqueue_round_persistent(bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb,
-                                     double dtb, int rk, cudaStream_t s) {
+RoundArgs<T> round_args(bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb, double dtb,
+                        int rk) {
   RoundArgs<T> a;
   a.g = p->geo<T>();
   for (int k = 0; k < 3; ++k) {
@@ -304,17 +312,19 @@ cudaError_t enqueue_round_persistent(bt_plan* p, const bt_state_in& in, const bt
   a.fy = (T*)p->face_y();
   a.nbb = nbb;
   a.rk = rk;
+  a.step0 = 0;
   a.dtb = dtb;
   a.bar = p->d_flags;
   a.err = (int*)(p->d_flags + 1);
   a.spin_limit = p->spin_limit;
-  cudaError_t e = cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned), s);
-  if (e != cudaSuccess) return e;
-  cudaEvent_t t1 = nullptr;
-  if ((e = p->time_begin(BT_KERNEL_ROUND, s, &t1)) != cudaSuccess) return e;
-  e = launch_round<T>(a, p->tile, p->max_ctas, s, &p->last_grid);
-  if (e != cudaSuccess) return e;
-  if (t1 && (e = cudaEventRecord(t1, s)) != cudaSuccess) return e;
+  return a;
+}
+
+// Halo fill of the result and the diagnostics of the last stage after a
+// persistent or resident round.
+template <typename T>
+cudaError_t round_epilogue(const RoundArgs<T>& a, const bt_state_out& out, int rk, cudaStream_t s) {
+  cudaError_t e;
   const Geo<T>& g = a.g;
   if (out.diag[0]) {
     T* const* L = rk == 2 ? a.y : a.z;
@@ -325,6 +335,145 @@ cudaError_t enqueue_round_persistent(bt_plan* p, const bt_state_in& in, const bt
     if ((e = launch_diag<T>(g, L[0], L[1], L[2], d, s)) != cudaSuccess) return e;
   }
   return launch_fill_halo<T>(g, a.x[0], a.x[1], a.x[2], s);
+}
+
+// Dependency lists of the resident kernel for tile shape c (see
+// bt_resident.cuh): for every tile, the tiles owning a cell it reads in
+// either phase of a stage -- the rectangle of 3 cells around the tile (halo
+// cells resolved to their two gather sources) and, along the face edges the
+// tile touches, the neighbour face's 6-point lines normal to the edge (their
+// halo points resolved likewise) -- made symmetric, without the tile itself.
+int build_resident_deps(bt_plan* p, TileCfg c) {
+  if (p->res_tile.ti == c.ti && p->res_tile.tj == c.tj && p->d_res) return BT_OK;
+  const int n = p->n, m = p->m, nh = p->nh;
+  const Tiling t = make_tiling(c, n);
+  const int ntiles = 6 * t.tiles_per_face();
+  auto owner = [&](long o) {
+    const int f = (int)(o / ((long)m * m));
+    const int r = (int)(o - (long)f * m * m), i = r / m, j = r % m;
+    return (f * t.nti + (i - kHalo) / t.ti) * t.ntj + (j - kHalo) / t.tj;
+  };
+  std::vector<std::vector<int>> dep(ntiles);
+  auto add = [&](int tile, int f, int i, int j) {
+    if (is_interior(i, j, m)) {
+      dep[tile].push_back(owner(cell(f, i, j, m)));
+    } else {
+      const int2 sx = p->h_src[(size_t)f * nh + halo_id(i, j, m)];
+      dep[tile].push_back(owner(sx.x));
+      dep[tile].push_back(owner(sx.y));
+    }
+  };
+  for (int f = 0; f < 6; ++f)
+    for (int ti = 0; ti < t.nti; ++ti)
+      for (int tj = 0; tj < t.ntj; ++tj) {
+        const int tile = (f * t.nti + ti) * t.ntj + tj;
+        const int i0 = kHalo + ti * t.ti, j0 = kHalo + tj * t.tj;
+        const int ni = std::min(t.ti, n - ti * t.ti), nj = std::min(t.tj, n - tj * t.tj);
+        for (int i = i0 - kHalo; i < i0 + ni + kHalo; ++i)
+          for (int j = j0 - kHalo; j < j0 + nj + kHalo; ++j) add(tile, f, i, j);
+        const bool touch[4] = {j0 + nj == m - kHalo, j0 == kHalo, i0 + ni == m - kHalo, i0 == kHalo};  // E W N S
+        for (int side = 0; side < 4; ++side) {
+          if (!touch[side]) continue;
+          const int r = p->route[f * 4 + side], nb = route_nb(r), ns = route_side(r);
+          const bool along_j = side == kS || side == kN;
+          const int k0 = along_j ? j0 - kHalo : i0 - kHalo, nk = along_j ? nj : ni;
+          for (int k = k0; k < k0 + nk; ++k) {
+            const int kk = route_rev(r) ? n - 1 - k : k;
+            for (int q = 0; q < 6; ++q) {
+              int i, j;
+              edge_point(ns, kk, q, m, i, j);
+              add(tile, nb, i, j);
+            }
+          }
+        }
+      }
+  for (int tile = 0; tile < ntiles; ++tile)
+    for (int d : std::vector<int>(dep[tile]))
+      if (d != tile) dep[d].push_back(tile);
+  std::vector<int> off(ntiles + 1, 0), idx;
+  for (int tile = 0; tile < ntiles; ++tile) {
+    std::vector<int>& v = dep[tile];
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    for (int d : v) {
+      if (d < 0 || d >= ntiles) return fail(BT_EINVAL, "resident mode: dependency outside the tile set");
+      if (d != tile) idx.push_back(d);
+    }
+    off[tile + 1] = (int)idx.size();
+  }
+  if (p->d_res) {
+    cudaFree(p->d_res);
+    p->d_res = nullptr;
+  }
+  const size_t words = (ntiles + 1) + idx.size() + ntiles + 1;
+  if (cudaMalloc(&p->d_res, words * sizeof(int)) != cudaSuccess)
+    return fail(BT_ENOMEM, "resident mode: dependency table allocation failed");
+  std::vector<int> blob(off);
+  blob.insert(blob.end(), idx.begin(), idx.end());
+  BT_CUDA(cudaMemcpy(p->d_res, blob.data(), blob.size() * sizeof(int), cudaMemcpyHostToDevice),
+          "resident mode: upload dependency table");
+  p->res_tile = c;
+  p->res_tiles = ntiles;
+  p->res_ndep = (int)idx.size();
+  return BT_OK;
+}
+
+// Resident mode: one cooperative launch with one CTA per tile runs every
+// phase of every substep (bt_resident.cuh); the plan's tile shape must be a
+// resident shape whose tiles all fit on the device at once.
+template <typename T>
+int enqueue_round_resident(bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb, double dtb,
+                           int rk, cudaStream_t s) {
+  if (!resident_tile_supported(p->tile))
+    return fail(BT_ENOTSUP, "bt_round: resident mode supports the tile shapes 8x16, 16x16 and 8x32");
+  int cap = 0;
+  cudaError_t e = resident_capacity<T>(p->tile, &cap);
+  if (e != cudaSuccess) return cuda_fail(e, "bt_round: resident occupancy");
+  const int ntiles = 6 * make_tiling(p->tile, p->n).tiles_per_face();
+  if (ntiles > cap)
+    return fail(BT_ENOTSUP, "bt_round: resident mode needs all " + std::to_string(ntiles) +
+                                " tiles on the GPU at once, " + std::to_string(cap) +
+                                " fit: use a larger tile or graph mode");
+  const int rc = build_resident_deps(p, p->tile);
+  if (rc != BT_OK) return rc;
+  RoundArgs<T> a = round_args<T>(p, in, out, nbb, dtb, rk);
+  ResSync rs;
+  rs.dep_off = p->d_res;
+  rs.dep_idx = p->d_res + ntiles + 1;
+  rs.flags = p->d_res + ntiles + 1 + p->res_ndep;
+  rs.abort = rs.flags + ntiles;
+  p->last_grid = ntiles;
+  for (int step0 = 0; step0 < nbb; step0 += kSubstepsPerLaunch) {
+    a.step0 = step0;
+    a.nbb = std::min(kSubstepsPerLaunch, nbb - step0);
+    if ((e = cudaMemsetAsync(rs.flags, 0, (ntiles + 1) * sizeof(int), s)) != cudaSuccess)
+      return cuda_fail(e, "bt_round: resident flags");
+    cudaEvent_t t1 = nullptr;
+    if ((e = p->time_begin(BT_KERNEL_ROUND, s, &t1)) != cudaSuccess) return cuda_fail(e, "bt_round: timing");
+    if ((e = launch_resident<T>(a, rs, p->tile, s)) != cudaSuccess) return cuda_fail(e, "bt_round: resident launch");
+    if (t1 && (e = cudaEventRecord(t1, s)) != cudaSuccess) return cuda_fail(e, "bt_round: timing");
+  }
+  if ((e = round_epilogue<T>(a, out, rk, s)) != cudaSuccess) return cuda_fail(e, "bt_round: halo fill");
+  return BT_OK;
+}
+
+// Persistent mode: one cooperative launch runs every phase of every substep.
+template <typename T>
+cudaError_t enqueue_round_persistent(bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb,
+                                     double dtb, int rk, cudaStream_t s) {
+  RoundArgs<T> a = round_args<T>(p, in, out, nbb, dtb, rk);
+  for (int step0 = 0; step0 < nbb; step0 += kSubstepsPerLaunch) {
+    a.step0 = step0;
+    a.nbb = std::min(kSubstepsPerLaunch, nbb - step0);
+    cudaError_t e = cudaMemsetAsync(p->d_flags, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t t1 = nullptr;
+    if ((e = p->time_begin(BT_KERNEL_ROUND, s, &t1)) != cudaSuccess) return e;
+    e = launch_round<T>(a, p->tile, p->max_ctas, s, &p->last_grid);
+    if (e != cudaSuccess) return e;
+    if (t1 && (e = cudaEventRecord(t1, s)) != cudaSuccess) return e;
+  }
+  return round_epilogue<T>(a, out, rk, s);
 }
 
 cudaError_t enqueue(const bt_plan* p, const bt_state_in& in, const bt_state_out& out, int nbb, double dtb,
@@ -412,6 +561,7 @@ int bt_plan_create(const bt_grid_desc* d, bt_plan** out) {
   cudaGetDevice(&p->device);
   p->field_elems = (size_t)6 * p->m * p->m;
   cudaError_t pe = p->dtype == BT_F64 ? prime_kernels<double>() : prime_kernels<float>();
+  if (pe == cudaSuccess) pe = p->dtype == BT_F64 ? prime_resident<double>() : prime_resident<float>();
   if (pe != cudaSuccess) {
     bt_plan_destroy(p);
     return cuda_fail(pe, "bt_plan_create: kernel attributes");
@@ -455,6 +605,7 @@ int bt_plan_destroy(bt_plan* p) {
   if (p->d_flags) cudaFree(p->d_flags);
   if (p->d_hsrc) cudaFree(p->d_hsrc);
   if (p->d_hw) cudaFree(p->d_hw);
+  if (p->d_res) cudaFree(p->d_res);
   delete p;
   return BT_OK;
 }
@@ -473,7 +624,7 @@ int bt_plan_set_tile(bt_plan* p, int ti, int tj) {
 
 int bt_plan_set_mode(bt_plan* p, int mode) {
   if (!p) return fail(BT_EINVAL, "bt_plan_set_mode: NULL plan");
-  if (mode != BT_MODE_STREAM && mode != BT_MODE_GRAPH && mode != BT_MODE_PERSISTENT)
+  if (mode != BT_MODE_STREAM && mode != BT_MODE_GRAPH && mode != BT_MODE_PERSISTENT && mode != BT_MODE_RESIDENT)
     return fail(BT_EINVAL, "bt_plan_set_mode: unknown mode");
   p->mode = mode;
   return BT_OK;
@@ -495,6 +646,9 @@ int bt_round(bt_plan* p, const bt_state_in* in, const bt_state_out* out, int nbb
     for (int k = 1; k < 10; ++k)
       if (!out->diag[k]) return fail(BT_EINVAL, "bt_round: diag outputs must be all set or diag[0] NULL");
   cudaStream_t s = (cudaStream_t)stream;
+  if (p->mode == BT_MODE_RESIDENT)
+    return p->dtype == BT_F64 ? enqueue_round_resident<double>(p, *in, *out, nbb, dtb, rk, s)
+                              : enqueue_round_resident<float>(p, *in, *out, nbb, dtb, rk, s);
   if (p->mode == BT_MODE_PERSISTENT) {
     cudaError_t e = p->dtype == BT_F64 ? enqueue_round_persistent<double>(p, *in, *out, nbb, dtb, rk, s)
                                        : enqueue_round_persistent<float>(p, *in, *out, nbb, dtb, rk, s);
@@ -589,6 +743,8 @@ int bt_check_device_error(bt_plan* p) {
     BT_CUDA(cudaMemset(p->d_flags + 1, 0, sizeof(unsigned)), "bt_check_device_error: clear flag");
     if (flags[1] & kErrBarrierTimeout)
       return fail(BT_EDEVICE, "persistent round: grid barrier wait exceeded its poll limit; the round was abandoned");
+    if (flags[1] & kErrNeighbourTimeout)
+      return fail(BT_EDEVICE, "resident round: a neighbour-tile wait exceeded its poll limit; the round was abandoned");
     return fail(BT_EDEVICE, "device error flag " + std::to_string(flags[1]));
   }
   return BT_OK;

@@ -95,7 +95,7 @@ struct StageIO {
 };
 
 // Error bits a kernel can raise in the plan's device flag.
-enum DeviceError { kErrBarrierTimeout = 1 };
+enum DeviceError { kErrBarrierTimeout = 1, kErrNeighbourTimeout = 2 };
 
 // Everything one persistent launch needs to run a whole round of one member.
 template <typename T>
@@ -106,6 +106,14 @@ struct Tiling {
   int ti, tj;        // tile extent (rows, cols)
   int nti, ntj;      // tiles per face along i and j
   __host__ __device__ int tiles_per_face() const { return nti * ntj; }
+};
+
+// Neighbour synchronisation of the tile-resident round kernel (bt_resident.cuh).
+struct ResSync {
+  const int* dep_off;  // (tiles + 1) offsets into dep_idx
+  const int* dep_idx;  // the tiles each tile waits for (symmetric relation)
+  int* flags;          // per tile: phases completed in this launch (zero at launch)
+  int* abort;          // set by a tile whose wait gave up; ends every other wait
 };
 
 template <typename T>
@@ -119,7 +127,8 @@ struct RoundArgs {
   T* z[3];         // second stage scratch (RK3)
   T* fx;           // face caches (phase H -> phase UV)
   T* fy;
-  int nbb, rk;
+  int nbb, rk;      // substeps of this launch, RK order
+  int step0;        // substep index of the launch's first substep within the round (0: reads x0/b0)
   double dtb;
   unsigned* bar;   // grid barrier counter, zero at launch
   int* err;        // device error flag

@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_round(RoundArgs<T> a) {
   unsigned gen = 0;
   EdgeCnt cnt;
   int P = 0;
-  if (threadIdx.x == 0) s_io[0] = round_stage(a, 0, 0);
+  if (threadIdx.x == 0) s_io[0] = round_stage(a, a.step0, 0);
   __syncthreads();
   // phase H of stage 0: the first tile's prologue
   Gather<T, TI, TJ, false> gh;
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_round(RoundArgs<T> a) {
       __syncthreads();
     }
     if (sg + 1 < nstage) {
-      if (threadIdx.x == 0) s_io[(sg + 1) & 1] = round_stage(a, (sg + 1) / nst, (sg + 1) % nst);
+      if (threadIdx.x == 0) s_io[(sg + 1) & 1] = round_stage(a, a.step0 + (sg + 1) / nst, (sg + 1) % nst);
       __syncthreads();
       if (t0 < ntiles) tile_h_pro<T, TI, TJ>(a.g, s_io[(sg + 1) & 1], tile_box(a.t, a.g.n, t0), sm, gh, cnt, P);
     }

@@ -30,6 +30,15 @@ cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, 
 // max_ctas > 0 caps the grid.  The grid size used is returned in *grid_out.
 template <typename T>
 cudaError_t launch_round(const RoundArgs<T>& a, TileCfg cfg, int max_ctas, cudaStream_t s, int* grid_out);
+// Tile-resident round (one CTA per tile, neighbour flags; bt_resident.cuh).
+bool resident_tile_supported(TileCfg c);
+template <typename T>
+cudaError_t prime_resident();
+// CTAs of the resident kernel for tile shape c that fit on the current device at once.
+template <typename T>
+cudaError_t resident_capacity(TileCfg c, int* ctas);
+template <typename T>
+cudaError_t launch_resident(const RoundArgs<T>& a, const ResSync& rs, TileCfg cfg, cudaStream_t s);
 // Materialise the halo cells of h (scalar) and/or (u, v) (vector) from their interiors.
 template <typename T>
 cudaError_t launch_fill_halo(const Geo<T>& g, T* h, T* u, T* v, cudaStream_t s);

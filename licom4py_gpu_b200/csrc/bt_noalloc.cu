@@ -10,22 +10,39 @@
 // library declares statically.
 //
 // The array (kScratchBytes, 6 MiB) belongs to every GPU that loads the library
-// and stays allocated until the process exits.  It holds, in this order: the
-// halo gather tables, the stage fields (3, or 6 for RK3) and the two face caches.
-// Float64 rounds fit up to N = 96 (RK2 and RK3); float32 somewhat more; larger
-// sizes are rejected with BT_EINVAL.
+// and stays allocated until the process exits.  It holds, in this order: a
+// status word, the halo gather tables, the stage fields (3, or 6 for RK3) and
+// the two face caches.  The largest sizes that fit: float64 N <= 116 (RK2) /
+// 99 (RK3), float32 N <= 165 (RK2) / 142 (RK3); larger sizes are rejected with
+// BT_EINVAL.
 //
 // Set-up: the first call on a device (with that device current) looks up the
 // array's device address with cudaGetSymbolAddress and sets the kernels'
-// shared-memory limits; make that first call before any stream capture.  Every
-// call reuses the same array and keeps whatever the previous call left there:
-// nothing in it has to start at zero (the tables are rebuilt and every cache
-// entry is written before it is read), but two calls whose work overlaps on
-// the GPU (different streams, or one device used from several threads) race
-// on it -- serialise them.
+// shared-memory limits; make that first call before any stream capture.
+//
+// Validation: the first call with a given set of constant pointers (per
+// device) checks on the device what bt_plan_create checks on the host -- every
+// k2e location the halo remap reads lies inside the band, and inner/outer are
+// the exact interior / halo masks -- and waits for the answer (a stream
+// synchronisation); tables that fail return BT_EINVAL / BT_ENOTSUP like
+// bt_plan_create.  Later calls with the same pointers skip the check, so the
+// tables must not change while they are in use (as for a plan).
+//
+// Every call reuses the same array and keeps whatever the previous call left
+// there: the status word is cleared before each check; nothing else has to
+// start at zero (the tables are rebuilt and every cache entry is written
+// before it is read), but two calls whose work overlaps on the GPU (different
+// streams, or one device used from several threads) race on it -- serialise
+// them.
+//
+// Tile shape: the round runs the 8 x 16 tiles, the shape with the most CTAs
+// at the sizes this entry point accepts (one full wave of 432 CTAs at N = 96,
+// three per SM) and the one the autotuner picks for float64 at N = 96; the
+// results are bitwise the same for every tile shape in float64.
 
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -37,6 +54,7 @@ namespace bt {
 namespace {
 
 constexpr size_t kScratchBytes = 6u << 20;  // 6 MiB
+constexpr size_t kStatusBytes = 256;          // status word of the table check, then the scratch proper
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
@@ -45,6 +63,16 @@ std::mutex g_setup_mutex;
 void* g_scratch_addr[kMaxDevices] = {};
 bool g_primed_f64[kMaxDevices] = {};
 bool g_primed_f32[kMaxDevices] = {};
+
+// The constant set last validated on each device (pointers, N, dtype).
+struct CheckedDesc {
+  bool valid = false;
+  int n = 0, dtype = 0;
+  const void* c[17] = {};
+};
+CheckedDesc g_checked[kMaxDevices];
+
+enum NoallocStatus : unsigned { kBadLocation = 1u, kBadMask = 2u };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -102,8 +130,8 @@ __device__ __forceinline__ long band_source(const RouteTable& rt, int f, int ti,
 
 // One thread per halo cell: two source cells and two weights (the linear
 // kinked -> extended remap along the band; corners take the band cell of row
-// 3 / M-4).  Location indices are clamped into the band so that inconsistent
-// tables cannot send a read out of bounds.
+// 3 / M-4).  Location indices are clamped into the band so that no read can go
+// out of bounds (k_check_tables has rejected tables that would need it).
 template <typename T>
 __global__ void k_build_halo(int n, const T* coef, const int* li, const int* lj, RouteTable rt, int2* src,
                              T* w) {
@@ -145,6 +173,66 @@ __global__ void k_build_halo(int n, const T* coef, const int* li, const int* lj,
   w[2 * k + 1] = coef[2 * ob + 1];
 }
 
+// The checks of bt_plan_create on the device, one thread per cell of the
+// (6, M, M) arrays: inner / outer must be the exact interior / halo masks
+// (kBadMask), and at a halo cell the k2e location the remap reads (loc_i
+// along the W/E bands, loc_j along the S/N bands, the band cell of row 3 /
+// M-4 at corners) must lie in [3, M-5] (kBadLocation).
+template <typename T>
+__global__ void k_check_tables(int n, const int* li, const int* lj, const T* inner, const T* outer,
+                               unsigned* status) {
+  const int m = n + 6;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 6 * m * m) return;
+  const int f = k / (m * m), r = k - f * m * m, i = r / m, j = r - (r / m) * m;
+  const bool in = is_interior(i, j, m);
+  const T want = in ? T(1) : T(0);
+  if (inner[k] != want || outer[k] != T(1) - want) atomicOr(status, (unsigned)kBadMask);
+  if (in) return;
+  int bi = i;
+  if ((i < kHalo || i >= m - kHalo) && (j < kHalo || j >= m - kHalo)) bi = i < kHalo ? kHalo : m - kHalo - 1;
+  const long ob = cell(f, bi, j, m);
+  const int loc = (j < kHalo || j >= m - kHalo) ? li[ob] : lj[ob];
+  if (loc < kHalo || loc > m - kHalo - 2) atomicOr(status, (unsigned)kBadLocation);
+}
+
+// Check the constant set once per device (see the file comment); waits for the result.
+template <typename T>
+int check_tables_once(unsigned char* base, const bt_grid_desc& d, cudaStream_t s) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return set_error(BT_ECUDA, "bt_round_noalloc: cudaGetDevice failed");
+  const void* cs[17] = {d.dzph_x, d.dzph_y, d.rdx, d.rdy, d.a_f, d.k2e_coef, d.loc_i_local, d.loc_j_local,
+                        d.a_c2l, d.a_l2c, d.inner, d.outer, d.a_gct, d.a_sina, d.rda, d.c_dy, d.d_dx};
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    const CheckedDesc& c = g_checked[dev];
+    if (c.valid && c.n == d.n && c.dtype == d.dtype && std::memcmp(c.c, cs, sizeof(cs)) == 0) return BT_OK;
+  }
+  unsigned* status = (unsigned*)base;
+  const int m = d.n + 6, total = 6 * m * m, th = 256;
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(unsigned), s);
+  if (e == cudaSuccess) {
+    k_check_tables<T><<<(total + th - 1) / th, th, 0, s>>>(d.n, d.loc_i_local, d.loc_j_local, (const T*)d.inner,
+                                                           (const T*)d.outer, status);
+    e = cudaGetLastError();
+  }
+  unsigned st = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&st, status, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return set_error(BT_ECUDA, std::string("bt_round_noalloc: table check: ") + cudaGetErrorString(e));
+  if (st & kBadMask)
+    return set_error(BT_ENOTSUP, "bt_round_noalloc: inner/outer must be the interior/halo masks of duogrid.py:159-190");
+  if (st & kBadLocation) return set_error(BT_EINVAL, "bt_round_noalloc: k2e location table out of range at a halo cell");
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  CheckedDesc& c = g_checked[dev];
+  c.valid = true;
+  c.n = d.n;
+  c.dtype = d.dtype;
+  std::memcpy(c.c, cs, sizeof(cs));
+  return BT_OK;
+}
+
 template <typename T>
 StageIO<T> io_of(const T* h, const T* u, const T* v, const T* hp, const T* up, const T* vp, T* ho, T* uo, T* vo,
                  T* fx, T* fy, double dt, double beta, int stored, int last) {
@@ -172,7 +260,8 @@ int run_noalloc(unsigned char* base, const bt_grid_desc& d, const bt_state_in& i
                 double dtb, int rk, cudaStream_t s) {
   const int n = d.n, m = n + 6, nh = halo_count(m);
   const size_t fe = (size_t)6 * m * m, face = (size_t)6 * (n + 1) * n * 3;
-  const size_t o_w = align256((size_t)6 * nh * sizeof(int2));
+  const size_t o_src = kStatusBytes;
+  const size_t o_w = o_src + align256((size_t)6 * nh * sizeof(int2));
   const size_t o_f = o_w + align256((size_t)6 * nh * 2 * sizeof(T));
   const int nfields = rk == 2 ? 3 : 6;
   const size_t o_fx = o_f + align256((size_t)nfields * fe * sizeof(T));
@@ -182,7 +271,9 @@ int run_noalloc(unsigned char* base, const bt_grid_desc& d, const bt_state_in& i
     return set_error(BT_EINVAL, "bt_round_noalloc: N = " + std::to_string(n) + " needs " + std::to_string(need) +
                                     " bytes of scratch, more than the library's fixed " +
                                     std::to_string(kScratchBytes) + "; use bt_plan_create/bt_round");
-  int2* hsrc = (int2*)base;
+  const int rc = check_tables_once<T>(base, d, s);
+  if (rc != BT_OK) return rc;
+  int2* hsrc = (int2*)(base + o_src);
   T* hw = (T*)(base + o_w);
   T* F = (T*)(base + o_f);
   T* fx = (T*)(base + o_fx);

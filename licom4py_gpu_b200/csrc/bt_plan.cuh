@@ -39,6 +39,13 @@ struct bt_plan {
   // graph cache
   cudaGraphExec_t gexec = nullptr;
   std::vector<uintptr_t> gkey;
+  // host copy of the halo gather sources (the resident mode's dependency lists are built from it)
+  std::vector<int2> h_src;
+  // resident mode: dependency lists and progress flags of the tile shape res_tile, one device block:
+  // dep_off [tiles + 1], dep_idx [ndep], flags [tiles], abort word
+  TileCfg res_tile{0, 0};
+  int* d_res = nullptr;
+  int res_tiles = 0, res_ndep = 0;
   // persistent mode: barrier counter + device error flag, options
   unsigned* d_flags = nullptr;  // [0] barrier counter, [1] error bits
   int max_ctas = 0;

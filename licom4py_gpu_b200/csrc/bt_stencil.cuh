@@ -118,7 +118,7 @@ __device__ __forceinline__ T contra(const Geo<T>& g, long o, T u, T v, int y) {
 // k-th of the 6 points (k = 0..5) on the line normal to ``side`` of a face that
 // straddles that side's C-grid edge face, at along-edge position kk.  The
 // edge face itself sits between points 2 and 3.
-__device__ __forceinline__ void edge_point(int side, int kk, int k, int m, int& i, int& j) {
+__host__ __device__ __forceinline__ void edge_point(int side, int kk, int k, int m, int& i, int& j) {
   switch (side) {
     case kS: i = k; j = kHalo + kk; break;
     case kN: i = m - 6 + k; j = kHalo + kk; break;
@@ -560,9 +560,26 @@ struct GatherSink {
   T* np;   // H: neighbour lines (contravariant normal velocity, h, depth)
   T* nh;
   T* ndz;
+  // tile-resident round only (RES): phase H also leaves the raw velocities of
+  // the region halo in phase UV's arrays, and phase UV blends with the stage
+  // h phase H staged
+  T* rv = nullptr;        // H: phase UV's raw v [VB]
+  T* ru = nullptr;        // H: phase UV's raw u [TI][RJ]
+  const T* hs = nullptr;  // UV: phase H's region h [RI][RJ]
 };
 
-template <typename T, int TI, int TJ, bool UV>
+// Shared-memory pointers of the tile-resident round kernel: phase H and phase
+// UV keep separate layouts, so constants and the face cache stay in place
+// for the whole round.
+template <typename T>
+struct ResSm {
+  T* uv;      // phase UV layout (constants, face cache, raw velocities of the stage)
+  T* pq;      // phase H face fluxes [FX + FY] (alias the metric block otherwise)
+  T* hs;      // phase H region h [RI][RJ]: the stage h of the fb blend in phase UV
+  int* items; // gather item scratch (kItemWords)
+};
+
+template <typename T, int TI, int TJ, bool UV, bool RES = false>
 struct Gather {
   using S = TileShape<TI, TJ>;
   // phase H gathers the region halo and the neighbour edge lines (9 items per
@@ -600,6 +617,15 @@ struct Gather {
   // read stays exact), and all loads precede the item's shared-memory stores.
   __device__ __forceinline__ void one(const Geo<T>& g, const StageIO<T>& io, const ItemCell& c, const Pull<T>& p,
                                       bool pull, const GatherSink<T>& k) {
+    if constexpr (UV && RES) {
+      // resident phase UV: the raw velocities and the stage h of the halo
+      // point were staged by phase H; only the new h is interpolated here
+      T hn = p.w0 * ((const T*)io.h_out)[p.s.x] + p.w1 * ((const T*)io.h_out)[p.s.y];
+      const int e = c.r * S::RJ + c.c;
+      if (io.beta != T(0.0)) hn = (T(1.0) - io.beta) * hn + io.beta * k.hs[e];  // fb_scheme
+      k.h[e] = hn;
+      return;
+    }
     const int o = c.o;
     const bool vpull = UV ? !io.stored_halo : pull;  // velocity interpolated (else read directly)
     const int sa = vpull ? p.s.x : o, sb = vpull ? p.s.y : o;
@@ -637,6 +663,12 @@ struct Gather {
           k.vb[c.r * TJ + (c.c - kHalo)] = ct;
         else
           k.hb[(c.r - kHalo) * S::RJ + c.c] = ct;
+        if constexpr (RES) {  // phase UV's raw (tangential-reading) velocity at the same point
+          if (c.kind < 2)
+            k.rv[c.r * TJ + (c.c - kHalo)] = v;
+          else
+            k.ru[(c.r - kHalo) * S::RJ + c.c] = u;
+        }
       } else {
         k.np[c.slot] = ct;
         if (want_h) {
@@ -776,12 +808,36 @@ struct LayoutH {
   }
 };
 
-// Phase H prologue: constants of the tile (cp.async, not yet awaited) and the
-// halo-gather descriptors.  Independent of the state, so it may run before the
-// previous phase has finished (programmatic launch, or before a grid barrier).
+template <typename T, int TI, int TJ>
+struct LayoutUV {
+  using S = TileShape<TI, TJ>;
+  T *s_v, *s_u, *s_hn, *s_hb, *s_g, *s_sn, *s_rda, *s_rdx, *s_rdy, *s_af, *s_xc, *s_cdy, *s_ku, *s_vx, *s_yc,
+      *s_ddx, *s_kv, *s_uy;
+  __device__ __forceinline__ explicit LayoutUV(T* sm) {
+    s_v = sm + S::uV;
+    s_u = sm + S::uU;
+    s_hn = sm + S::uHN;
+    s_hb = sm + S::uHB;
+    s_g = sm + S::uG;
+    s_sn = sm + S::uSN;
+    s_rda = sm + S::uRDA;
+    s_rdx = sm + S::uRDX;
+    s_rdy = sm + S::uRDY;
+    s_af = sm + S::uAF;
+    s_xc = sm + S::uXC;
+    s_cdy = sm + S::uCDY;
+    s_ku = sm + S::uKU;
+    s_vx = sm + S::uVX;
+    s_yc = sm + S::uYC;
+    s_ddx = sm + S::uDDX;
+    s_kv = sm + S::uKV;
+    s_uy = sm + S::uUY;
+  }
+};
+
+// Phase H constants of the tile (cp.async, not yet awaited).
 template <typename T, int TI, int TJ, bool FULL>
-__device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                             Gather<T, TI, TJ, false>& gat, EdgeCnt& cnt, int& P) {
+__device__ __forceinline__ void tile_h_consts(const Geo<T>& g, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
   const LayoutH<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
@@ -838,12 +894,29 @@ __device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& 
     cp_async_t(L.s_dzy + r * (TJ + 1) + TJ, g.dzph_y + o);
     cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + o);
   }
+}
+
+// Halo-gather descriptors of a tile phase (edge tiles; P = 0 for full tiles).
+template <typename T, int TI, int TJ, bool FULL, bool UV, bool RES>
+__device__ __forceinline__ void tile_desc(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
+                                          Gather<T, TI, TJ, UV, RES>& gat, EdgeCnt& cnt, int& P, int* items) {
   if (FULL) {
     P = 0;
   } else {
-    P = edge_count(b, m, g.route, cnt);
-    if (P > 0) gat.descriptors(g, io, b, cnt, P, reinterpret_cast<int*>(sm + S::kWordsH));
+    P = edge_count(b, g.m, g.route, cnt);
+    if (P > 0) gat.descriptors(g, io, b, cnt, P, items);
   }
+}
+
+// Phase H prologue: constants of the tile (cp.async, not yet awaited) and the
+// halo-gather descriptors.  Independent of the state, so it may run before the
+// previous phase has finished (programmatic launch, or before a grid barrier).
+template <typename T, int TI, int TJ, bool FULL>
+__device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                             Gather<T, TI, TJ, false>& gat, EdgeCnt& cnt, int& P) {
+  using S = TileShape<TI, TJ>;
+  tile_h_consts<T, TI, TJ, FULL>(g, b, sm);
+  tile_desc<T, TI, TJ, FULL, false, false>(g, io, b, gat, cnt, P, reinterpret_cast<int*>(sm + S::kWordsH));
 }
 
 // Phase H of one x face or y face: C-grid normal velocity (remap.py:41-55)
@@ -887,15 +960,25 @@ __device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, c
 }
 
 // Phase H of one tile: writes the new h on the tile's interior cells.
-template <typename T, int TI, int TJ, bool FULL>
+// RES (tile-resident round): the constants are already in shared memory, the
+// face fluxes get their own area, and the face cache and the raw velocities
+// of the region go to phase UV's layout (rs.uv) instead of global memory.
+template <typename T, int TI, int TJ, bool FULL, bool RES = false>
 __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                              Gather<T, TI, TJ, false>& gat, const EdgeCnt& cnt, int P) {
+                                              Gather<T, TI, TJ, false, RES>& gat, const EdgeCnt& cnt, int P,
+                                              const ResSm<T>& rs = ResSm<T>{}) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
   static_assert(6 * TI <= kTileThreads, "one side point per thread");
   const int m = g.m, n = g.n, f = b.f, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
   const int ni = FULL ? TI : b.ni, nj = FULL ? TJ : b.nj;
-  const LayoutH<T, TI, TJ> L(sm);
+  LayoutH<T, TI, TJ> L(sm);
+  const LayoutUV<T, TI, TJ> U(RES ? rs.uv : sm);  // RES only
+  if constexpr (RES) {
+    L.s_P = rs.pq;
+    L.s_Q = rs.pq + S::FX;
+  }
+  int* const items = RES ? rs.items : reinterpret_cast<int*>(sm + S::kWordsH);
   // state of the thread's interior region points and base h of its cells, into registers
   T hv[S::KV], uv[S::KV], vv[S::KV], hpc[S::KC];
   T hs = T(0.0), us = T(0.0), vs = T(0.0);
@@ -930,9 +1013,14 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
     const int a = sl + k * S::NS;
     if (q < nj && a < ni) hpc[k] = io.hp[ov + (a + kHalo) * m];
   }
-  if (!FULL && P > 0)
-    gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_h, L.s_uc, L.s_vc, L.s_np, L.s_nh, L.s_ndz},
-                reinterpret_cast<const int*>(sm + S::kWordsH));
+  if (!FULL && P > 0) {
+    GatherSink<T> sink{L.s_h, L.s_uc, L.s_vc, L.s_np, L.s_nh, L.s_ndz};
+    if constexpr (RES) {
+      sink.rv = U.s_v;
+      sink.ru = U.s_u;
+    }
+    gat.sources(g, io, b, cnt, P, sink, items);
+  }
   cp_async_wait_all();
   __syncthreads();
 
@@ -944,9 +1032,14 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
       const int p = r * TJ + q;
       const T* G = L.s_g + 4 * p;
       const T sn = L.s_sn[p], u = uv[k], v = vv[k];
+      const bool row = r >= kHalo && r < ni + kHalo;
       L.s_h[r * RJ + q + kHalo] = hv[k];
       L.s_uc[p] = (G[0] * u + G[1] * v) * sn;
-      if (r >= kHalo && r < ni + kHalo) L.s_vc[(r - kHalo) * RJ + q + kHalo] = (G[2] * u + G[3] * v) * sn;
+      if (row) L.s_vc[(r - kHalo) * RJ + q + kHalo] = (G[2] * u + G[3] * v) * sn;
+      if constexpr (RES) {  // phase UV's raw velocities (tangential reconstructions)
+        U.s_v[p] = v;
+        if (row) U.s_u[(r - kHalo) * RJ + q + kHalo] = u;
+      }
     }
   }
   if (!FULL) {
@@ -964,6 +1057,7 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
         const T sn = L.s_sn[p];
         L.s_h[r * RJ + q + kHalo] = h;
         L.s_uc[p] = (G[0] * u + G[1] * v) * sn;
+        if constexpr (RES) U.s_v[p] = v;
       }
     }
   }
@@ -972,6 +1066,7 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
     const T sn = L.s_sn[S::VB + t6];
     L.s_h[(sr + kHalo) * RJ + scc] = hs;
     L.s_vc[sr * RJ + scc] = (G[2] * us + G[3] * vs) * sn;
+    if constexpr (RES) U.s_u[sr * RJ + scc] = us;
   }
   __syncthreads();
 
@@ -985,11 +1080,12 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
         const int side =
             FULL ? -1 : ((a == 0 && b.i0 == kHalo) ? kS : ((a == ni && b.i0 + ni == m - kHalo) ? kN : -1));
         const int e = a * TJ + q;
-        T* fc = (a < ni || side == kN)
-                    ? io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n)
-                    : nullptr;
+        T* fc = RES ? U.s_xc + e
+                    : ((a < ni || side == kN) ? io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n)
+                                              : nullptr);
         const T fl = face_h<T>(io, L.s_h + a * RJ + q + kHalo, RJ, L.s_uc + a * TJ + q, TJ, side,
-                               (side == kS ? 0 : 1) * S::EW + q, L.s_dzx[e], L.s_np, L.s_nh, L.s_ndz, fc, PF);
+                               (side == kS ? 0 : 1) * S::EW + q, L.s_dzx[e], L.s_np, L.s_nh, L.s_ndz, fc,
+                               RES ? S::FX : PF);
         L.s_P[e] = fl * L.s_cdy[e];
       }
     }
@@ -1010,11 +1106,12 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
     const int side =
         FULL ? -1 : ((qq == 0 && b.j0 == kHalo) ? kW : ((qq == nj && b.j0 + nj == m - kHalo) ? kE : -1));
     const int e = r * (TJ + 1) + qq;
-    T* fc = (qq < nj || side == kE)
-                ? io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n)
-                : nullptr;
+    T* fc = RES ? U.s_yc + e
+                : ((qq < nj || side == kE) ? io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n)
+                                           : nullptr);
     const T fl = face_h<T>(io, L.s_h + (r + kHalo) * RJ + qq, 1, L.s_vc + r * RJ + qq, 1, side,
-                           (side == kW ? 2 : 3) * S::EW + r, L.s_dzy[e], L.s_np, L.s_nh, L.s_ndz, fc, PF);
+                           (side == kW ? 2 : 3) * S::EW + r, L.s_dzy[e], L.s_np, L.s_nh, L.s_ndz, fc,
+                           RES ? S::FY : PF);
     L.s_Q[e] = fl * L.s_ddx[e];
   }
   __syncthreads();
@@ -1034,37 +1131,9 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
 }
 
 // ---- phase UV -----------------------------------------------------------------
-template <typename T, int TI, int TJ>
-struct LayoutUV {
-  using S = TileShape<TI, TJ>;
-  T *s_v, *s_u, *s_hn, *s_hb, *s_g, *s_sn, *s_rda, *s_rdx, *s_rdy, *s_af, *s_xc, *s_cdy, *s_ku, *s_vx, *s_yc,
-      *s_ddx, *s_kv, *s_uy;
-  __device__ __forceinline__ explicit LayoutUV(T* sm) {
-    s_v = sm + S::uV;
-    s_u = sm + S::uU;
-    s_hn = sm + S::uHN;
-    s_hb = sm + S::uHB;
-    s_g = sm + S::uG;
-    s_sn = sm + S::uSN;
-    s_rda = sm + S::uRDA;
-    s_rdx = sm + S::uRDX;
-    s_rdy = sm + S::uRDY;
-    s_af = sm + S::uAF;
-    s_xc = sm + S::uXC;
-    s_cdy = sm + S::uCDY;
-    s_ku = sm + S::uKU;
-    s_vx = sm + S::uVX;
-    s_yc = sm + S::uYC;
-    s_ddx = sm + S::uDDX;
-    s_kv = sm + S::uKV;
-    s_uy = sm + S::uUY;
-  }
-};
-
-// Phase UV prologue: cell and face constants (cp.async) and the halo-gather descriptors.
+// Phase UV cell and face constants of the tile (cp.async, not yet awaited).
 template <typename T, int TI, int TJ, bool FULL>
-__device__ __forceinline__ void tile_uv_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                              Gather<T, TI, TJ, true>& gat, EdgeCnt& cnt, int& P) {
+__device__ __forceinline__ void tile_uv_consts(const Geo<T>& g, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
   const LayoutUV<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
@@ -1101,17 +1170,25 @@ __device__ __forceinline__ void tile_uv_pro_t(const Geo<T>& g, const StageIO<T>&
     const int r = east_row();
     cp_async_t(L.s_ddx + r * (TJ + 1) + TJ, g.d_dx + cell32(b.f, b.i0 + r, b.j0 + TJ, m));
   }
-  if (FULL) {
-    P = 0;
-  } else {
-    P = edge_count(b, m, g.route, cnt);
-    if (P > 0) gat.descriptors(g, io, b, cnt, P, reinterpret_cast<int*>(sm + S::kWordsUV));
-  }
 }
 
+// Phase UV prologue: cell and face constants (cp.async) and the halo-gather descriptors.
 template <typename T, int TI, int TJ, bool FULL>
+__device__ __forceinline__ void tile_uv_pro_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
+                                              Gather<T, TI, TJ, true>& gat, EdgeCnt& cnt, int& P) {
+  using S = TileShape<TI, TJ>;
+  tile_uv_consts<T, TI, TJ, FULL>(g, b, sm);
+  tile_desc<T, TI, TJ, FULL, true, false>(g, io, b, gat, cnt, P, reinterpret_cast<int*>(sm + S::kWordsUV));
+}
+
+// RES (tile-resident round): the constants, the face cache and the raw
+// velocities of the region are already in shared memory (left there by phase
+// H of the same stage), and the stage h of the fb blend is phase H's region h
+// (rs.hs); only the new h of the region is read from global memory.
+template <typename T, int TI, int TJ, bool FULL, bool RES = false>
 __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
-                                               Gather<T, TI, TJ, true>& gat, const EdgeCnt& cnt, int P) {
+                                               Gather<T, TI, TJ, true, RES>& gat, const EdgeCnt& cnt, int P,
+                                               const ResSm<T>& rs = ResSm<T>{}) {
   using S = TileShape<TI, TJ>;
   constexpr int RJ = S::RJ;
   static_assert(6 * TI <= kTileThreads, "one side point per thread");
@@ -1121,9 +1198,11 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
   const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
   const T* hn_src = (const T*)io.h_out;
   const int PF = 6 * (n + 1) * n;
+  const T* const hb = RES ? rs.hs : L.s_hb;  // stage h of the blend, region layout [RI][RJ]
+  const int* const items = RES ? rs.items : reinterpret_cast<const int*>(sm + S::kWordsUV);
 
   // face caches of this stage (written by phase H) -> shared memory
-  if (q < nj) {
+  if (!RES && q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
       const int a = sl + k * S::NS;
@@ -1138,6 +1217,7 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
   }
 #pragma unroll
   for (int k = 0; k <= S::KC; ++k) {
+    if (RES) break;
     int r, qq;
     if (k < S::KC) {
       r = sl + k * S::NS;
@@ -1170,9 +1250,11 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
       const int e = r * RJ + q + kHalo;
       const int o = ov + r * m;
       cp_async_t(L.s_hn + e, hn_src + o);
-      if (blend) cp_async_t(L.s_hb + e, io.h + o);
-      cp_async_t(L.s_v + r * TJ + q, io.v + o);
-      if (row) cp_async_t(L.s_u + (r - kHalo) * RJ + q + kHalo, io.u + o);
+      if (!RES) {
+        if (blend) cp_async_t(L.s_hb + e, io.h + o);
+        cp_async_t(L.s_v + r * TJ + q, io.v + o);
+        if (row) cp_async_t(L.s_u + (r - kHalo) * RJ + q + kHalo, io.u + o);
+      }
     }
   }
   if (!FULL) {
@@ -1183,7 +1265,13 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
       const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
       if (q < nj && r < ni + 6 && ec.row_staged(i, m) && !(i >= kHalo && i < m - kHalo)) {
         const int e = r * RJ + q + kHalo;
-        T hn = fetch_s(hn_src, g, f, i, b.j0 + q, 0), u, v;
+        T hn = fetch_s(hn_src, g, f, i, b.j0 + q, 0);
+        if (RES) {  // raw velocities and the stage h staged by phase H
+          if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * hb[e];
+          L.s_hn[e] = hn;
+          continue;
+        }
+        T u, v;
         fetch_v(io.u, io.v, g, f, i, b.j0 + q, io.stored_halo, u, v);
         if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * fetch_s(io.h, g, f, i, b.j0 + q, io.stored_halo);
         L.s_hn[e] = hn;
@@ -1201,8 +1289,14 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
     if (side_in) {
       const int o = cell32(f, b.i0 + sr, sj, m);
       cp_async_t(L.s_hn + e, hn_src + o);
-      if (blend) cp_async_t(L.s_hb + e, io.h + o);
-      cp_async_t(L.s_u + sr * RJ + scc, io.u + o);
+      if (!RES) {
+        if (blend) cp_async_t(L.s_hb + e, io.h + o);
+        cp_async_t(L.s_u + sr * RJ + scc, io.u + o);
+      }
+    } else if (RES) {
+      T hn = fetch_s(hn_src, g, f, b.i0 + sr, sj, 0);
+      if (blend) hn = (T(1.0) - io.beta) * hn + io.beta * hb[e];
+      L.s_hn[e] = hn;
     } else {
       T hn = fetch_s(hn_src, g, f, b.i0 + sr, sj, 0), u, v;
       fetch_v(io.u, io.v, g, f, b.i0 + sr, sj, io.stored_halo, u, v);
@@ -1219,9 +1313,11 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
       vpc[k] = io.vp[ov + (a + kHalo) * m];
     }
   }
-  if (!FULL && P > 0)
-    gat.sources(g, io, b, cnt, P, GatherSink<T>{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr},
-                reinterpret_cast<const int*>(sm + S::kWordsUV));
+  if (!FULL && P > 0) {
+    GatherSink<T> sink{L.s_hn, L.s_v, L.s_u, nullptr, nullptr, nullptr};
+    sink.hs = hb;
+    gat.sources(g, io, b, cnt, P, sink, items);
+  }
   cp_async_wait_all();
   __syncthreads();
   if (blend) {  // fb_scheme, barotr_pure.py:52-54, on the points staged by cp.async
@@ -1230,12 +1326,12 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
       const int r = sl + k * S::NS, i = b.i0 - kHalo + r;
       if (q < nj && r < ni + 6 && (FULL || (i >= kHalo && i < m - kHalo))) {
         const int e = r * RJ + q + kHalo;
-        L.s_hn[e] = (T(1.0) - io.beta) * L.s_hn[e] + io.beta * L.s_hb[e];
+        L.s_hn[e] = (T(1.0) - io.beta) * L.s_hn[e] + io.beta * hb[e];
       }
     }
     if (side_pt && side_in) {
       const int e = (sr + kHalo) * RJ + scc;
-      L.s_hn[e] = (T(1.0) - io.beta) * L.s_hn[e] + io.beta * L.s_hb[e];
+      L.s_hn[e] = (T(1.0) - io.beta) * L.s_hn[e] + io.beta * hb[e];
     }
     __syncthreads();
   }
@@ -1419,7 +1515,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned& gen, int* 
   return s_ok != 0;
 }
 
-// Stage pointers of (substep, stage) of a round; mirrors the host schedule.
+// Stage pointers of (substep, stage) of a round, ``step`` counted from the
+// round's first substep; mirrors the host schedule.
 // Fields are picked with constant indexes only, so the kernel arguments are
 // never addressed (which would copy them to local memory).
 template <typename T>

@@ -24,7 +24,8 @@ DIAG_NAMES = ("celerity_x", "celerity_y", "ub_ct", "vb_ct", "ub_cx", "ub_cy", "v
               "advx", "advy")
 _INT_CONSTS = ("loc_i_local", "loc_j_local")
 
-_MODES = {"stream": N.BT_MODE_STREAM, "graph": N.BT_MODE_GRAPH, "persistent": N.BT_MODE_PERSISTENT}
+_MODES = {"stream": N.BT_MODE_STREAM, "graph": N.BT_MODE_GRAPH, "persistent": N.BT_MODE_PERSISTENT,
+          "resident": N.BT_MODE_RESIDENT}
 
 
 def _ptr(t: Optional[torch.Tensor]):
@@ -112,12 +113,13 @@ class BtPlan:
         self.set_option(N.BT_OPT_MAX_CTAS, n)
 
     def set_spin_limit(self, polls: int) -> None:
-        """Persistent mode: polls a grid-barrier wait may take before the round is abandoned."""
+        """Persistent / resident mode: polls a grid-barrier or neighbour-tile wait may take
+        before the round is abandoned."""
         self.set_option(N.BT_OPT_SPIN_LIMIT, polls)
 
     def enable_kernel_timing(self, on: bool = True) -> None:
-        """Bracket the round kernel (persistent mode) or each phase kernel (stream
-        mode) with CUDA events on its stream; resets the record."""
+        """Bracket the round kernel (persistent / resident mode) or each phase kernel
+        (stream mode) with CUDA events on its stream; resets the record."""
         self.set_option(N.BT_OPT_KERNEL_TIMING, 1 if on else 0)
 
     KERNELS = {"round": N.BT_KERNEL_ROUND, "phase_h": N.BT_KERNEL_PHASE_H, "phase_uv": N.BT_KERNEL_PHASE_UV}

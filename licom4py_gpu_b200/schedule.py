@@ -110,14 +110,27 @@ class Timer:
         self.prev_dt = self.current
 
 
+def _namelist_value(namelist, name: str):
+    """A derived namelist value: the reference's private field ``_<name>`` if the
+    object has it, else the public attribute ``name``; AttributeError if neither."""
+    for attr in ("_" + name, name):
+        if hasattr(namelist, attr):
+            return getattr(namelist, attr)
+    raise AttributeError(f"namelist has neither _{name} nor {name}")
+
+
 class Schedule:
     """Global scheduler (schedule.py:200-313): configure once, then run in chunks."""
 
     @classmethod
     def configure(cls, namelist, momentum, routines: Optional[list] = None) -> None:
-        cls.current_time = Timer(getattr(namelist, "start_datetime", _dt.datetime(2000, 1, 1)),
-                                 namelist.baroclinic_dt)
-        cls.total_baroclinic_steps = int(namelist.total_baroclinic_steps)
+        """``namelist`` is the reference's ``Namelist`` (its derived values are the
+        private ``_start_datetime`` / ``_total_baroclinic_steps`` fields,
+        readnamelist/time_data.py:61, namelist_data.py:56, read as at
+        schedule.py:216-218) or any object with the public names
+        ``start_datetime`` / ``total_baroclinic_steps`` (this package's ``Namelist``)."""
+        cls.current_time = Timer(_namelist_value(namelist, "start_datetime"), namelist.baroclinic_dt)
+        cls.total_baroclinic_steps = int(_namelist_value(namelist, "total_baroclinic_steps"))
         cls.routines = ["barotropic", "baroclinic", "tracer"] if routines is None else routines
         diag_freq = getattr(namelist, "diag_freq", None)
         cls.diag_interval = (int(3600 / namelist.baroclinic_dt * diag_freq)

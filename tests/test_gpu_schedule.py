@@ -81,3 +81,21 @@ def test_schedule_run_w92_steady_state(capsys):
     state = [s0["h0"], s0["h0"], s0["ub"], s0["vb"], s0["ub"], s0["vb"]] + [np.zeros((6, m, m))] * 17
     want = O.rk2_core(state, consts, 24 * 6, 600.0)
     np.testing.assert_array_equal(mom.h0.cpu().numpy(), want[0])
+
+
+def test_schedule_configure_with_reference_namelist():
+    """Schedule.configure/run driven by an object shaped like the reference's Namelist
+    (private _start_datetime / _total_baroclinic_steps only)."""
+    from test_schedule_host import RefLikeNamelist
+    Duogrid.configure(24, depth=5600.0)
+    mom = Momentum(Namelist(barotropic_dt=600.0, baroclinic_dt=3600.0, integration_days=1.0, nx=24),
+                   case="w92case2")
+    mom.verbose = False
+    ref_nl = RefLikeNamelist(baroclinic_dt=3600, diag_freq=12, async_threads=2, _total_baroclinic_steps=24)
+    schedule.Schedule.configure(ref_nl, mom)
+    assert schedule.Schedule.total_baroclinic_steps == 24
+    schedule.Schedule.run(mom)
+    reports = schedule.Schedule.reports
+    assert len(reports) == 1 + 2  # initial + every 12 h of one day
+    assert "2001-03-04-05" in reports[0] and "2001-03-05-05" in reports[-1]
+

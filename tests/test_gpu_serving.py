@@ -60,3 +60,18 @@ def test_requests_arriving_later_join_running_rounds(geo):
     assert stats["requests"] == 2
     assert reqs[1].t_admit >= reqs[1].arrival and reqs[1].t_done < reqs[0].t_done
     assert stats["p99_s"] >= stats["p50_s"] > 0
+
+
+@pytest.mark.parametrize("n,seed,amp", [(12, 5, 1.0), (24, 77, 0.37), (48, 1234, 1.9)])
+def test_device_initial_state_equals_seeded_field_generator(n, seed, amp, geo):
+    """The serving path's device-built initial state (HarmonicBasis) is the seeded
+    harmonic field of fields.harmonic_state (h RMS = amplitude, u/v RMS = 0.3 x
+    amplitude), up to float64 rounding of the reordered sums: 1e-12 relative."""
+    from licom4py_gpu_b200.fields import harmonic_state
+    from licom4py_gpu_b200.serving import HarmonicBasis
+    basis = HarmonicBasis(geo, torch.device("cuda"))
+    got = basis.state(Request(rid=0, n=n, nsub=1, seed=seed, amplitude=amp), torch.float64)
+    want = harmonic_state(geo.grid(n), seed, amp, 0.3 * amp)
+    for t, key in zip(got, ("h0", "ub", "vb")):
+        err = rel_err(t.cpu().numpy(), want[key])
+        assert err <= 1e-12, f"C{n} seed {seed} {key}: rel err {err:.2e}"
