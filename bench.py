@@ -61,7 +61,7 @@ def parse_args():
     p.add_argument("--nbb", type=int, default=1000)
     p.add_argument("--depth", type=float, default=5000.0)
     p.add_argument("--seed", type=int, default=1)
-    p.add_argument("--mode", default="auto", choices=["auto", "persistent", "graph", "stream"])
+    p.add_argument("--mode", default="auto", choices=["auto", "resident", "persistent", "graph", "stream"])
     p.add_argument("--tile", default="auto")
     p.add_argument("--cpu-substeps", type=int, default=60,
                    help="substeps of the bounded CPU baseline sample")
@@ -73,6 +73,8 @@ def parse_args():
                    help="skip the layered forms (precision at C384, batched ensemble, serving)")
     p.add_argument("--serving-requests", type=int, default=100,
                    help="requests of the Poisson serving stream in the bounded serving sample")
+    p.add_argument("--no-oracle-check", action="store_true",
+                   help="skip the float64 oracle run of the full timed round (error_vs_oracle)")
     return p.parse_args()
 
 
@@ -110,11 +112,15 @@ def max_over_ranks(x, world):
     return replicas.max_over_ranks(x)
 
 
+GEOMETRY_CACHE = {}  # resolution -> "hit" / "generated" (duogrid_C{N}.npz cache)
+
+
 def build_problem(n, depth, seed):
     from licom4py_gpu_b200 import duogrid_gen
     from licom4py_gpu_b200.duogrid import make_consts
     from licom4py_gpu_b200.fields import cfl_dtb, harmonic_state
-    grid = duogrid_gen.generate(n)
+    grid, hit = duogrid_gen.load_or_generate(n)
+    GEOMETRY_CACHE[n] = "hit" if hit else "generated"
     consts = make_consts(grid, depth)
     st = harmonic_state(grid, seed)
     dtb = cfl_dtb(grid, depth)
@@ -191,6 +197,90 @@ def cpu_baseline(consts, st, dtb, n, substeps):
     return {"value": cells * substeps / dt, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"C{n} float64, {substeps} RK2 substeps from the same initial state "
                       f"({dt:.1f} s, single-threaded NumPy oracle)"}
+
+
+def l2_copy_gbs(dev, reps=50):
+    """Device copy bandwidth of an L2-resident buffer (16 MiB read + 16 MiB written per
+    copy), bytes moved / time: the L2 figure the C48-C96 rounds are set against."""
+    import torch
+    src = torch.ones(4 << 20, dtype=torch.float32, device=dev)
+    dst = torch.empty_like(src)
+    for _ in range(5):
+        dst.copy_(src)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        dst.copy_(src)
+    b.record()
+    torch.cuda.synchronize()
+    return 2 * src.numel() * 4 * reps / (a.elapsed_time(b) * 1e-3) / 1e9
+
+
+def _oracle_round(n, depth, seed, nbb):
+    """The oracle's float64 h0, ub, vb after the full round of the timed workload."""
+    from oracle import barotr_np as O
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
+    _, consts, st, dtb = build_problem(n, depth, seed)
+    m = n + 6
+    state = [st["h0"], st["h0"], st["ub"], st["vb"], st["ub"], st["vb"]] + [np.zeros((6, m, m))] * 17
+    out = O.rk2_core(state, consts, nbb, dtb)
+    return out[0], out[2], out[3]
+
+
+class OracleCheck:
+    """Part of the CPU-baseline leg: the float64 oracle runs the timed workload's
+    full round (every substep, same inputs) in one spawned host process while the
+    GPU legs run, and the GPU results of the timed runs are compared with it."""
+
+    def __init__(self, n, depth, seed, nbb):
+        import multiprocessing as mp
+        self.nbb = nbb
+        self.pool = mp.get_context("spawn").Pool(1)
+        self.job = self.pool.apply_async(_oracle_round, (n, depth, seed, nbb))
+
+    def compare(self, results, timeout_s=900.0):
+        """results: {label: {"h0": t, "ub": t, "vb": t}} of device tensors; per label
+        and field the relative L2 and max-norm error over the interior, and whether
+        the field equals the oracle bit for bit."""
+        try:
+            want = self.job.get(timeout=timeout_s)
+        except Exception as e:  # a report, not a failure of the bench
+            return {"error": f"oracle run did not finish: {type(e).__name__}"}
+        finally:
+            self.pool.terminate()
+        rep = {"substeps": self.nbb}
+        for label, res in results.items():
+            r = {}
+            for key, ref in zip(("h0", "ub", "vb"), want):
+                got = res[key].double().cpu().numpy()
+                a, b = got[:, 3:-3, 3:-3], ref[:, 3:-3, 3:-3]
+                r[key] = {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                          "rel_linf": float(np.abs(a - b).max() / np.abs(b).max()),
+                          "bitwise": bool(np.array_equal(got, ref))}
+            rep[label] = r
+        return rep
+
+
+def _oracle_requests(depth, items):
+    """The oracle's float64 h0 for each (n, substeps, seed, amplitude) request of the
+    serving stream (initial state as fields.harmonic_state, dtb at CFL 0.5)."""
+    from oracle import barotr_np as O
+    from licom4py_gpu_b200 import duogrid_gen
+    from licom4py_gpu_b200.duogrid import make_consts
+    from licom4py_gpu_b200.fields import cfl_dtb, harmonic_state
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
+    res = []
+    for n, nsub, seed, amp in items:
+        grid = duogrid_gen.load_or_generate(n)[0]
+        consts = make_consts(grid, depth)
+        st = harmonic_state(grid, seed, amp, 0.3 * amp)
+        m = n + 6
+        state = [st["h0"], st["h0"], st["ub"], st["vb"], st["ub"], st["vb"]] + [np.zeros((6, m, m))] * 17
+        res.append(O.rk2_core(state, consts, nsub, cfl_dtb(grid, depth))[0])
+    return res
 
 
 _REF_PROBLEM = None
@@ -275,7 +365,7 @@ def form_precision(dev, depth, peak, seeds=8, nsub=2000):
     from licom4py_gpu_b200.momentum import conservation
     from licom4py_gpu_b200.plan import BtPlan
     n = 384
-    grid = duogrid_gen.generate(n)
+    grid = duogrid_gen.load_or_generate(n)[0]
     consts = make_consts(grid, depth)
     dtb = cfl_dtb(grid, depth)
     rda = {}
@@ -405,11 +495,18 @@ def form_serving(dev, depth, count):
     import torch
     from licom4py_gpu_b200.ensemble import Geometry
     from licom4py_gpu_b200.serving import BarotropicServer, Request, poisson_mix, run_fifo
+    import multiprocessing as mp
     geo = Geometry(depth, device=dev)
     for n in (48, 96, 192, 384):
         geo.plan(n, torch.float32)
         geo.dtb(n)
     keep = ("p50_s", "p99_s", "mean_s", "max_s", "requests", "wall_s", "cell_updates_per_s")
+    # part of the CPU-baseline leg: the float64 oracle runs the 8 smallest requests of
+    # the stream in a spawned host process while the GPU serves
+    smallest = sorted(poisson_mix(count=count, rate=200.0, seed=0), key=lambda r: r.cell_updates)[:8]
+    pool = mp.get_context("spawn").Pool(1)
+    oracle_job = pool.apply_async(_oracle_requests, (depth, [(r.n, r.nsub, r.seed, r.amplitude)
+                                                             for r in smallest]))
     out = {}
     first = None
     for rate, orders in ((200.0, ("fifo", "shortest")), (20.0, ("fifo",))):
@@ -447,6 +544,16 @@ def form_serving(dev, depth, count):
     out["workload"] = (f"first {count} requests of the 10k-request Poisson stream (seed 0), at 200 and at "
                        f"20 requests/s, float32, RK2")
     out["h_rel_l2_vs_f64_smallest8"] = err64
+    try:
+        want = oracle_job.get(timeout=900)
+        served = {r.rid: r for r in first}
+        out["h_rel_l2_vs_oracle_smallest8"] = max(
+            float(np.linalg.norm(served[r.rid].result["h0"][:, 3:-3, 3:-3] - w[:, 3:-3, 3:-3]) /
+                  np.linalg.norm(w[:, 3:-3, 3:-3])) for r, w in zip(smallest, want))
+    except Exception as e:  # a report, not a failure of the bench
+        out["h_rel_l2_vs_oracle_smallest8"] = f"oracle run did not finish: {type(e).__name__}"
+    finally:
+        pool.terminate()
     return out
 
 
@@ -462,6 +569,10 @@ def run_ours(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     grid, consts, st, dtb = build_problem(args.n, args.depth, args.seed + rank)
+    # the oracle's run of the same full round, in a spawned host process meanwhile
+    oracle = (OracleCheck(args.n, args.depth, args.seed, args.nbb)
+              if rank == 0 and world == 1 and not args.no_oracle_check else None)
+    checked = {}
     n, m, nbb = args.n, args.n + 6, args.nbb
     cells = 6 * n * n
 
@@ -510,12 +621,12 @@ def run_ours(args, world, rank, local):
     sampler = ClockSampler(local)
     with sampler:
         ms, (kms, klaunch) = timed_rounds(plan, ins64, out, args.steps, args.warmup,
-                                          kernel_timing=(mode == "persistent"))
+                                          kernel_timing=(mode in ("persistent", "resident")))
     clocks = sampler.summary()
     ms = max_over_ranks(ms, world)
     ms_per_step = ms / args.steps
     value = world * cells * nbb * args.steps / (ms * 1e-3)
-    launches_per_step = {"persistent": 4, "graph": 4 * nbb + 3, "stream": 4 * nbb + 3}[mode]
+    launches_per_step = {"resident": 4, "persistent": 4, "graph": 4 * nbb + 3, "stream": 4 * nbb + 3}[mode]
 
     # roofline of the dominant kernel
     peaks = {}
@@ -561,7 +672,27 @@ def run_ours(args, world, rank, local):
                 "alg_bytes_per_launch": alg, "launches_timed": nl,
                 "share_of_phase_time": {k: res[k][0] / tot for k in res}}
 
-    roofline = kernel_roofline(n, torch.float64, tile, nbb, consts, st, dtb)
+    if mode in ("resident", "persistent") and klaunch > 0:
+        # the round is one kernel: its event-timed launches in the headline run itself
+        alg = B_ALG_WORDS * 8 * cells * nbb
+        achieved = alg / (kms / klaunch * 1e-3) / 1e9
+        l2 = l2_copy_gbs(dev)
+        kname = "k_resident" if mode == "resident" else "k_round"
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", f"{kname}_c{n}_f64.json")
+        if os.path.exists(tfile):
+            try:
+                traffic = json.load(open(tfile)).get("dram_bytes_per_launch")
+            except (OSError, ValueError):
+                traffic = None
+        roofline = {"bound": "l2" if 41 * 8 * 6 * (n + 6) ** 2 < 64e6 else "hbm",
+                    "kernel": f"{kname}<double,{tile[0]},{tile[1]}>", "achieved": achieved, "peak": peak,
+                    "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                    "launch_us": 1e3 * kms / klaunch, "launches_timed": klaunch, "launches_per_step": 1,
+                    "alg_bytes_per_launch": alg, "timed_in": "headline run (events around the round kernel)",
+                    "l2_copy_gbs": l2, "frac_of_l2_copy": achieved / l2 if l2 else None}
+    else:
+        roofline = kernel_roofline(n, torch.float64, tile, nbb, consts, st, dtb)
     round_roofline = {"achieved": B_ALG_WORDS * 8 * cells * nbb / (ms_per_step * 1e-3) / 1e9,
                       "peak": peak, "unit": "GB/s",
                       "frac": B_ALG_WORDS * 8 * cells * nbb / (ms_per_step * 1e-3) / 1e9 / peak,
@@ -609,6 +740,7 @@ def run_ours(args, world, rank, local):
         p32 = make_plan(torch.float32, mode, tile)
         out32 = {k: p32.empty_field() for k in ("h0", "ub", "vb") + DIAG_NAMES}
         ms32, _ = timed_rounds(p32, ins32, out32, args.steps, args.warmup)
+        checked["f32"] = out32
         ms32 = max_over_ranks(ms32, world)
         h64 = out["h0"][:, 3:-3, 3:-3]
         h32 = out32["h0"][:, 3:-3, 3:-3].double()
@@ -618,7 +750,7 @@ def run_ours(args, world, rank, local):
         p32.close()
         # round execution modes (CUDA graph vs persistent vs stream), float64
         modes = {}
-        for md in ("persistent", "graph", "stream"):
+        for md in ("resident", "persistent", "graph", "stream"):
             pm = make_plan(torch.float64, md, tile)
             steps = max(2, args.steps // 2)
             msm, _ = timed_rounds(pm, ins64, out, steps, 2)
@@ -654,6 +786,9 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(consts, st, dtb, n, args.cpu_substeps)
+    if oracle is not None:
+        checked["f64"] = out
+        extras["error_vs_oracle"] = oracle.compare(checked)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -662,6 +797,7 @@ def run_ours(args, world, rank, local):
                 "data": "synthetic: seeded spherical harmonics l=1..8 (h 1 m RMS, u/v 0.3 m/s RMS) over H=5000 m",
                 "config": {"workload": f"C{n} plain drop-in RK2 round, {nbb} substeps per step, float64",
                            "n": n, "nbb": nbb, "rk": 2, "dtb_s": dtb, "mode": mode, "tile": list(tile),
+                           "geometry": {f"C{k}": v for k, v in GEOMETRY_CACHE.items()},
                            "parallelism": f"replicas x{world}",
                            "l2": "flushed between steps (512 MiB write outside the timed windows); "
                                  "within a step the member's working set stays L2-resident"},

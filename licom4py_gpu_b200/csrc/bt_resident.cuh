@@ -35,6 +35,14 @@
 
 namespace bt {
 
+// Resident CTAs per SM the kernel is compiled for (register cap 65536 / (256 *
+// blocks)).  The float64 layouts of the larger tiles (16 x 16, 8 x 32: over
+// 100 KB) fit only two CTAs per SM anyway, so they get the registers of two.
+template <typename T, int TI, int TJ>
+struct ResBlocks {
+  static constexpr int value = (sizeof(T) == 8 && TI * TJ > 128) ? 2 : 3;
+};
+
 // Shared-memory layout of a resident CTA (words of T): phase H layout, phase
 // H face fluxes, phase UV layout, then the gather item scratch (ints).
 template <typename T, int TI, int TJ>
@@ -128,7 +136,7 @@ __device__ __forceinline__ bool res_stage(const RoundArgs<T>& a, const ResSync& 
 
 // One CTA per tile (face-major order); the grid is exactly the tile count.
 template <typename T, int TI, int TJ>
-__global__ void __launch_bounds__(kTileThreads, 3) k_resident(RoundArgs<T> a, ResSync rsy) {
+__global__ void __launch_bounds__(kTileThreads, ResBlocks<T, TI, TJ>::value) k_resident(RoundArgs<T> a, ResSync rsy) {
   using RL = ResLayout<T, TI, TJ>;
   using S = TileShape<TI, TJ>;
   extern __shared__ __align__(16) unsigned char smraw[];

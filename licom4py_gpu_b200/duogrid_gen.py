@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from typing import Dict, Iterable, Optional
+from typing import Dict, Iterable, Optional, Tuple
 
 import numpy as np
 
@@ -112,6 +112,45 @@ def generate(nx: int, fields: Optional[Iterable[str]] = None,
 def npz_name(nx: int) -> str:
     """File name of the serialised grid (src/initial_field/main.py:96)."""
     return f"duogrid_C{nx}.npz"
+
+
+def cache_dir() -> str:
+    """Directory of the per-resolution NPZ cache: ``$LICOM_BT_FIELD_DIR``, else
+    ``~/.cache/licom4py_gpu_b200/field`` (the reference keeps its files in ``field/``)."""
+    return os.environ.get("LICOM_BT_FIELD_DIR",
+                          os.path.join(os.path.expanduser("~"), ".cache", "licom4py_gpu_b200", "field"))
+
+
+def load_or_generate(nx: int, directory: Optional[str] = None) -> Tuple[Dict[str, np.ndarray], bool]:
+    """The C{nx} geometry from ``duogrid_C{nx}.npz`` in ``directory`` (default
+    :func:`cache_dir`), generating and writing the file on the first request.
+
+    The reference generates the file once (``make field``,
+    src/initial_field/main.py:81-98) and every run loads it
+    (src/licom/duogrid/duogrid.py:58-59); this does both, so repeated runs at
+    one resolution skip the generator.  Returns (fields, cache_hit).  A file
+    that lacks an essential field or has the wrong shape is regenerated.
+    """
+    d = directory if directory is not None else cache_dir()
+    path = os.path.join(d, npz_name(nx))
+    m = int(nx) + 6
+    if os.path.exists(path):
+        try:
+            with np.load(path) as z:
+                data = {k: z[k] for k in z.files}
+            if ESSENTIAL_FIELDS <= set(data) and data["rdx"].shape == (6, m, m):
+                return data, True
+        except (OSError, ValueError, KeyError):
+            pass
+    data = generate(nx)
+    try:
+        os.makedirs(d, exist_ok=True)
+        tmp = f"{path}.{os.getpid()}.tmp.npz"
+        np.savez(tmp, **data)
+        os.replace(tmp, path)
+    except OSError:
+        pass  # a read-only cache directory only costs the regeneration next time
+    return data, False
 
 
 class DuogridFieldGenerator:

@@ -65,7 +65,7 @@ class Geometry:
 
     def grid(self, n: int) -> dict:
         if n not in self._grids:
-            self._grids[n] = duogrid_gen.generate(n)
+            self._grids[n] = duogrid_gen.load_or_generate(n)[0]
         return self._grids[n]
 
     def plan(self, n: int, dtype: torch.dtype) -> BtPlan:

@@ -19,7 +19,8 @@ outputs are committed as ``tests/golden/*.npz``; the tests never import the
 reference.  Each fixture records the SHA-256 of the float64 constants it was
 made with so the tests can check that the generator still reproduces them.
 
-Usage:  python tests/golden/make_golden.py [--ref PATH_TO_REFERENCE]
+Usage:  python tests/golden/make_golden.py --ref PATH_TO_REFERENCE
+        (or set LICOM_REFERENCE_ROOT to the reference checkout)
 """
 
 from __future__ import annotations
@@ -193,9 +194,12 @@ def gen_core(ref_root, out, name, n, nbb, seed, rk=2, base_seed=None, keep_input
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--ref", default="/root/reference")
+    p.add_argument("--ref", default=os.environ.get("LICOM_REFERENCE_ROOT"),
+                   help="root of the reference checkout (default: $LICOM_REFERENCE_ROOT)")
     p.add_argument("--out", default=HERE)
     a = p.parse_args()
+    if not a.ref:
+        p.error("give --ref PATH_TO_REFERENCE or set LICOM_REFERENCE_ROOT")
     gen_halo(a.ref, a.out)
     gen_stage(a.ref, a.out)
     gen_core(a.ref, a.out, "rk2_c8.npz", n=8, nbb=4, seed=1)
