@@ -151,6 +151,9 @@ int batch_round(bt_batch* b, const bt_member* mem, int count, int rk, cudaStream
     if ((e = cudaMemsetAsync(b->d_flags, 0, sizeof(unsigned), s)) != cudaSuccess)
       return bcuda(e, "bt_batch_round: reset barrier");
     e = launch_batch_round<T>(a, b->tile, o_tile[count], b->max_ctas, s, &b->last_grid);
+    if (e == cudaErrorInvalidValue)
+      return bfail(BT_EINVAL, "bt_batch_round: persistent mode takes at most 2^31 barrier arrivals per round "
+                              "(2 x stages x substeps x CTAs): use fewer substeps per round or stream mode");
     if (e != cudaSuccess) return bcuda(e, "bt_batch_round: persistent launch");
   } else {
     const int nst = rk == 2 ? 2 : 3;

@@ -297,6 +297,9 @@ cudaError_t launch_batch_round_tile(BatchArgs<T> a, int max_tiles, int max_ctas,
   int grid = std::min(per_sm * sms, max_tiles);
   if (max_ctas > 0) grid = std::min(grid, max_ctas);
   if (grid < 1) return cudaErrorInvalidConfiguration;
+  // the grid barrier counts arrivals in 31 bits: (phases + 2 end sweeps) x CTAs must stay below 2^31
+  const long long arrivals = ((long long)a.max_nbb * (a.rk == 2 ? 2 : 3) * 2 + 2) * grid;
+  if (arrivals >= (1ll << 31)) return cudaErrorInvalidValue;
   if (grid_out) *grid_out = grid;
   void* args[] = {&a};
   return cudaLaunchCooperativeKernel((const void*)k_batch_round<T, TI, TJ>, dim3(grid), dim3(kTileThreads), args,
