@@ -73,6 +73,8 @@ def parse_args():
                    help="skip the layered forms (precision at C384, batched ensemble, serving)")
     p.add_argument("--serving-requests", type=int, default=100,
                    help="requests of the Poisson serving stream in the bounded serving sample")
+    p.add_argument("--only-form", default=None, choices=["precision", "ensemble", "serving"],
+                   help="run one layered form alone on one GPU and print its figures as one JSON line")
     p.add_argument("--no-oracle-check", action="store_true",
                    help="skip the float64 oracle run of the full timed round (error_vs_oracle)")
     return p.parse_args()
@@ -808,10 +810,33 @@ def run_ours(args, world, rank, local):
     plan.close()
 
 
+def run_form(args):
+    """One layered form alone (N = 1), e.g. the serving stream at its configured size."""
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs") or 6650.0
+    if args.only_form == "precision":
+        res = form_precision(dev, args.depth, peak)
+    elif args.only_form == "ensemble":
+        res = form_ensemble(dev, args.depth)
+    else:
+        res = form_serving(dev, args.depth, args.serving_requests)
+    print(json.dumps({"form": args.only_form, "n_gpus": 1, **res}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.case_only:
         run_case(args)
+        return
+    if args.only_form:
+        run_form(args)
         return
     world, rank, local = dist_setup(args)
     try:

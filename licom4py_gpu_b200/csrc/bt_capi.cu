@@ -405,7 +405,8 @@ int build_resident_deps(bt_plan* p, TileCfg c) {
     cudaFree(p->d_res);
     p->d_res = nullptr;
   }
-  const size_t words = (ntiles + 1) + idx.size() + ntiles + 1;
+  // offsets, lists, up to one line of padding, then one line per tile's flag and one for the abort word
+  const size_t words = (ntiles + 1) + idx.size() + kResFlagStride + (size_t)(ntiles + 1) * kResFlagStride;
   if (cudaMalloc(&p->d_res, words * sizeof(int)) != cudaSuccess)
     return fail(BT_ENOMEM, "resident mode: dependency table allocation failed");
   std::vector<int> blob(off);
@@ -440,13 +441,15 @@ int enqueue_round_resident(bt_plan* p, const bt_state_in& in, const bt_state_out
   ResSync rs;
   rs.dep_off = p->d_res;
   rs.dep_idx = p->d_res + ntiles + 1;
-  rs.flags = p->d_res + ntiles + 1 + p->res_ndep;
-  rs.abort = rs.flags + ntiles;
+  // flags start on a 128-byte boundary, one line per tile, the abort word on the line after them
+  const size_t flag0 = ((size_t)ntiles + 1 + p->res_ndep + kResFlagStride - 1) / kResFlagStride * kResFlagStride;
+  rs.flags = p->d_res + flag0;
+  rs.abort = rs.flags + (size_t)ntiles * kResFlagStride;
   p->last_grid = ntiles;
   for (int step0 = 0; step0 < nbb; step0 += kSubstepsPerLaunch) {
     a.step0 = step0;
     a.nbb = std::min(kSubstepsPerLaunch, nbb - step0);
-    if ((e = cudaMemsetAsync(rs.flags, 0, (ntiles + 1) * sizeof(int), s)) != cudaSuccess)
+    if ((e = cudaMemsetAsync(rs.flags, 0, ((size_t)ntiles + 1) * kResFlagStride * sizeof(int), s)) != cudaSuccess)
       return cuda_fail(e, "bt_round: resident flags");
     cudaEvent_t t1 = nullptr;
     if ((e = p->time_begin(BT_KERNEL_ROUND, s, &t1)) != cudaSuccess) return cuda_fail(e, "bt_round: timing");

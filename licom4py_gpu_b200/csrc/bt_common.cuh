@@ -109,10 +109,14 @@ struct Tiling {
 };
 
 // Neighbour synchronisation of the tile-resident round kernel (bt_resident.cuh).
+// Each tile's flag has a 128-byte line of its own (kResFlagStride ints): the
+// flags are polled continuously, and packing them would send every poll of
+// the grid to a handful of L2 lines.
+constexpr int kResFlagStride = 32;
 struct ResSync {
   const int* dep_off;  // (tiles + 1) offsets into dep_idx
   const int* dep_idx;  // the tiles each tile waits for (symmetric relation)
-  int* flags;          // per tile: phases completed in this launch (zero at launch)
+  int* flags;          // tile t's flag at flags[t * kResFlagStride]: phases completed in this launch
   int* abort;          // set by a tile whose wait gave up; ends every other wait
 };
 

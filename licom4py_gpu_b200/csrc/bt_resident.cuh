@@ -55,13 +55,11 @@ struct ResLayout {
 };
 
 // Publish that this CTA has completed ``phases`` phases: every thread's global
-// stores are ordered before the flag by the barrier and the release store.
+// stores are ordered before the flag by the barrier and the (cumulative)
+// release store.
 __device__ __forceinline__ void res_publish(int* flag, int phases) {
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(flag), "r"(phases) : "memory");
-  }
+  if (threadIdx.x == 0) asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(flag), "r"(phases) : "memory");
 }
 
 // Wait until every dependency of ``tile`` has completed ``need`` phases.  The
@@ -75,7 +73,7 @@ __device__ __forceinline__ bool res_wait(const ResSync& s, int tile, int need, i
     const int b = s.dep_off[tile], e = s.dep_off[tile + 1];
     int ok = 1;
     for (int k = b + lane; k < e && ok; k += 32) {
-      const int* fp = s.flags + s.dep_idx[k];
+      const int* fp = s.flags + s.dep_idx[k] * kResFlagStride;
       long long polls = 0;
       while (true) {
         int seen;
@@ -117,7 +115,7 @@ __device__ __forceinline__ bool res_stage(const RoundArgs<T>& a, const ResSync& 
     tile_desc<T, TI, TJ, FULL, false, true>(a.g, io, b, gat, cnt, P, rs.items);
     if (done > 0 && !res_wait(rsy, tile, done, a.err, a.spin_limit)) return false;
     tile_h_main_t<T, TI, TJ, FULL, true>(a.g, io, b, sm, gat, cnt, P, rs);
-    res_publish(rsy.flags + tile, done + 1);
+    res_publish(rsy.flags + tile * kResFlagStride, done + 1);
   }
   {
     Gather<T, TI, TJ, true, true> gat;
@@ -128,8 +126,8 @@ __device__ __forceinline__ bool res_stage(const RoundArgs<T>& a, const ResSync& 
       cp_async_wait_all();
       return false;
     }
-    tile_uv_main_t<T, TI, TJ, FULL, true>(a.g, io, b, sm, gat, cnt, P, rs);
-    res_publish(rsy.flags + tile, done + 2);
+    tile_uv_main_t<T, TI, TJ, FULL, true>(a.g, io, b, rs.uv, gat, cnt, P, rs);  // phase UV's own layout
+    res_publish(rsy.flags + tile * kResFlagStride, done + 2);
   }
   return true;
 }

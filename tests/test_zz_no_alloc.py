@@ -13,6 +13,7 @@ them, and that a call after a warm-up call leaves the device's free memory
 unchanged.  This file is named to be collected last.
 """
 import ctypes
+import gc
 
 import numpy as np
 import pytest
@@ -85,12 +86,13 @@ def test_noalloc_allocates_no_device_memory(grids):
     dtb = cfl_dtb(g, 5000.0)
     _noalloc_round(plan, ins, 2, dtb, 2)  # warm-up: set-up, table check, lazy kernel loading
     out = {k: plan.empty_field() for k in ("h0", "ub", "vb") + DIAG_NAMES}
+    gc.collect()  # plans of earlier tests free their memory when collected, not during the call
     torch.cuda.synchronize()
     torch_before, free_before = torch.cuda.memory_allocated(), torch.cuda.mem_get_info()[0]
     _noalloc_round(plan, ins, 3, dtb, 2, out=out)
     torch.cuda.synchronize()
     assert torch.cuda.memory_allocated() == torch_before
-    assert torch.cuda.mem_get_info()[0] == free_before
+    assert torch.cuda.mem_get_info()[0] >= free_before  # nothing was allocated on the device
     plan.close()
 
 
