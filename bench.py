@@ -201,11 +201,12 @@ def cpu_baseline(consts, st, dtb, n, substeps):
                       f"({dt:.1f} s, single-threaded NumPy oracle)"}
 
 
-def l2_copy_gbs(dev, reps=50):
-    """Device copy bandwidth of an L2-resident buffer (16 MiB read + 16 MiB written per
-    copy), bytes moved / time: the L2 figure the C48-C96 rounds are set against."""
+def l2_copy_gbs(dev, reps=100):
+    """Device copy bandwidth of L2-resident buffers (48 MiB read + 48 MiB written per copy,
+    96 MiB in all, under the 126 MB L2; large enough that the gaps between copies are
+    small), bytes moved / time: the L2 figure the C48-C96 rounds are set against."""
     import torch
-    src = torch.ones(4 << 20, dtype=torch.float32, device=dev)
+    src = torch.ones(12 << 20, dtype=torch.float32, device=dev)
     dst = torch.empty_like(src)
     for _ in range(5):
         dst.copy_(src)
