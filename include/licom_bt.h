@@ -197,7 +197,7 @@ int bt_conservation(int n, int dtype, const void* h, const void* u, const void* 
  * and the halo tables are rebuilt on the device each call, stream-ordered.
  * All scratch lives in one 6 MiB array the library declares statically
  * (held by every GPU that loads the library until exit).  Largest sizes:
- * float64 N <= 116 (rk 2) / 99 (rk 3), float32 N <= 165 (rk 2) / 142 (rk 3);
+ * float64 N <= 112 (rk 2) / 96 (rk 3), float32 N <= 160 (rk 2) / 136 (rk 3);
  * larger sizes return BT_EINVAL.  The first call on a device sets up the
  * array's address and must come before any stream capture.  The first call
  * with a given set of constant pointers on a device checks the tables as

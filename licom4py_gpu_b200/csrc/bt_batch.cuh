@@ -25,8 +25,7 @@ struct MemberDesc {
   T* x[3];         // output state (written by the last stage of each substep)
   T* y[3];         // stage scratch
   T* z[3];         // second stage scratch (RK3)
-  T* fx;           // face caches
-  T* fy;
+  T* fx;           // face cache blocks
   T* diag[10];     // STATE_KEYS[6:16] outputs, all null when not wanted
   double dtb;
   int geo;         // index into the call's geometry table

@@ -28,8 +28,8 @@ constexpr int kMaxGeo = 16;
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Member scratch layout: stage fields Y (3) [+ Z (3) for RK3], then the x and
-// y face caches, every part 256-byte aligned.
+// Member scratch layout: stage fields Y (3) [+ Z (3) for RK3], then the face
+// cache blocks, every part 256-byte aligned.
 struct ScratchLayout {
   size_t field, face, total;
   int nfields;
@@ -37,9 +37,9 @@ struct ScratchLayout {
 ScratchLayout scratch_layout(const bt_plan* p, int rk) {
   ScratchLayout L;
   L.field = align256(p->field_elems * p->esize());
-  L.face = align256(p->face_elems() * p->esize());
+  L.face = align256(face_cache_elems(p->n) * p->esize());
   L.nfields = rk == 3 ? 6 : 3;
-  L.total = L.nfields * L.field + 2 * L.face;
+  L.total = L.nfields * L.field + L.face;
   return L;
 }
 
@@ -113,7 +113,6 @@ int batch_round(bt_batch* b, const bt_member* mem, int count, int rk, cudaStream
       md.z[k] = rk == 3 ? (T*)(sc + (3 + k) * L.field) : nullptr;
     }
     md.fx = (T*)(sc + L.nfields * L.field);
-    md.fy = (T*)(sc + L.nfields * L.field + L.face);
     const bool dg = u.out.diag[0] != nullptr;
     for (int k = 0; k < 10; ++k) md.diag[k] = dg ? (T*)u.out.diag[k] : nullptr;
     md.dtb = u.dtb;

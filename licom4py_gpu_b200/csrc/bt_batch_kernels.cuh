@@ -70,7 +70,6 @@ __device__ StageIO<T> member_stage(const MemberDesc<T>& d, int rk, int step, int
   io.u_out = out[1];
   io.v_out = out[2];
   io.fx = d.fx;
-  io.fy = d.fy;
   double dt;
   if (rk == 2) {
     dt = st == 0 ? d.dtb / 2.0 : d.dtb;

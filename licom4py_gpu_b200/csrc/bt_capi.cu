@@ -187,7 +187,6 @@ StageIO<T> stage_io(const bt_plan* p, const T* h, const T* u, const T* v, const 
                     T* ho, T* uo, T* vo, double dt, double beta, int stored, int last) {
   StageIO<T> io;
   io.fx = (T*)p->face_x();
-  io.fy = (T*)p->face_y();
   io.h = h;
   io.u = u;
   io.v = v;
@@ -309,7 +308,6 @@ RoundArgs<T> round_args(bt_plan* p, const bt_state_in& in, const bt_state_out& o
   a.x[1] = (T*)out.ub;
   a.x[2] = (T*)out.vb;
   a.fx = (T*)p->face_x();
-  a.fy = (T*)p->face_y();
   a.nbb = nbb;
   a.rk = rk;
   a.step0 = 0;
@@ -574,7 +572,7 @@ int bt_plan_create(const bt_grid_desc* d, bt_plan** out) {
     bt_plan_destroy(p);
     return rc;
   }
-  const size_t bytes = p->scratch_elems() * p->esize();
+  const size_t bytes = p->scratch_bytes();
   cudaError_t e = cudaMalloc(&p->scratch, bytes);
   if (e != cudaSuccess) {
     bt_plan_destroy(p);
@@ -794,7 +792,7 @@ long long bt_plan_get_info(bt_plan* p, int key) {
   if (!p) return -1;
   switch (key) {
     case BT_INFO_LAST_GRID: return p->last_grid;
-    case BT_INFO_SCRATCH_BYTES: return (long long)(p->scratch_elems() * p->esize());
+    case BT_INFO_SCRATCH_BYTES: return (long long)p->scratch_bytes();
     default: return -1;
   }
 }

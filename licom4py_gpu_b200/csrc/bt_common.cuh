@@ -86,8 +86,9 @@ struct StageIO {
   T* h_out;     // stage outputs (interior cells only)
   T* u_out;
   T* v_out;
-  T* fx;        // face cache, x faces (6, N+1, N, 3): averaged normal velocity,
-  T* fy;        // its viscous correction, celerity flux; y faces (6, N, N+1, 3)
+  T* fx;        // face cache, one block per tile (bt_stencil.cuh, TileShape::fW): for every x face
+                // and y face of the tile its averaged normal velocity, viscous correction and
+                // celerity flux, written by phase H, read by phase UV of the same tile
   T dt;
   T beta;
   int stored_halo;  // 1: the inputs' halo cells hold valid values (first stage of a round)
@@ -129,8 +130,7 @@ struct RoundArgs {
   T* x[3];         // output / running state
   T* y[3];         // stage scratch
   T* z[3];         // second stage scratch (RK3)
-  T* fx;           // face caches (phase H -> phase UV)
-  T* fy;
+  T* fx;           // face cache blocks (phase H -> phase UV)
   int nbb, rk;      // substeps of this launch, RK order
   int step0;        // substep index of the launch's first substep within the round (0: reads x0/b0)
   double dtb;

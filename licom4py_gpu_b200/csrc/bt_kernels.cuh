@@ -121,6 +121,21 @@ bool tile_cfg_supported(TileCfg c) {
          (c.tj == 16 && (c.ti == 8 || c.ti == 16));
 }
 
+namespace {
+template <int TI, int TJ>
+size_t face_cache_elems_tile(int n) {
+  const size_t nti = (n + TI - 1) / TI, ntj = (n + TJ - 1) / TJ;
+  return 6 * nti * ntj * (size_t)TileShape<TI, TJ>::fW;
+}
+}  // namespace
+
+size_t face_cache_elems(int n) {
+  const size_t s[6] = {face_cache_elems_tile<7, 32>(n), face_cache_elems_tile<8, 32>(n),
+                       face_cache_elems_tile<15, 32>(n), face_cache_elems_tile<16, 32>(n),
+                       face_cache_elems_tile<8, 16>(n), face_cache_elems_tile<16, 16>(n)};
+  return *std::max_element(s, s + 6);
+}
+
 Tiling make_tiling(TileCfg c, int n) {
   Tiling t;
   t.ti = c.ti;

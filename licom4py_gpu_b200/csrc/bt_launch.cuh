@@ -17,6 +17,9 @@ struct TileCfg {
 
 // Tile shapes compiled into the library (rows x columns of interior cells).
 bool tile_cfg_supported(TileCfg c);
+// Elements of the face cache blocks of one member at n cells per face edge,
+// enough for every supported tile shape (the plan's tile can change later).
+size_t face_cache_elems(int n);
 Tiling make_tiling(TileCfg c, int n);
 
 // Set kernel attributes (dynamic shared memory opt-in) for the current device.

@@ -12,8 +12,8 @@
 // The array (kScratchBytes, 6 MiB) belongs to every GPU that loads the library
 // and stays allocated until the process exits.  It holds, in this order: a
 // status word, the halo gather tables, the stage fields (3, or 6 for RK3) and
-// the two face caches.  The largest sizes that fit: float64 N <= 116 (RK2) /
-// 99 (RK3), float32 N <= 165 (RK2) / 142 (RK3); larger sizes are rejected with
+// the face cache blocks of the 8 x 16 tiles.  The largest sizes that fit: float64 N <= 112 (RK2) /
+// 96 (RK3), float32 N <= 160 (RK2) / 136 (RK3); larger sizes are rejected with
 // BT_EINVAL.
 //
 // Set-up: the first call on a device (with that device current) looks up the
@@ -235,7 +235,7 @@ int check_tables_once(unsigned char* base, const bt_grid_desc& d, cudaStream_t s
 
 template <typename T>
 StageIO<T> io_of(const T* h, const T* u, const T* v, const T* hp, const T* up, const T* vp, T* ho, T* uo, T* vo,
-                 T* fx, T* fy, double dt, double beta, int stored, int last) {
+                 T* fx, double dt, double beta, int stored, int last) {
   StageIO<T> io;
   io.h = h;
   io.u = u;
@@ -247,7 +247,6 @@ StageIO<T> io_of(const T* h, const T* u, const T* v, const T* hp, const T* up, c
   io.u_out = uo;
   io.v_out = vo;
   io.fx = fx;
-  io.fy = fy;
   io.dt = (T)dt;
   io.beta = (T)beta;
   io.stored_halo = stored;
@@ -259,14 +258,15 @@ template <typename T>
 int run_noalloc(unsigned char* base, const bt_grid_desc& d, const bt_state_in& in, const bt_state_out& out, int nbb,
                 double dtb, int rk, cudaStream_t s) {
   const int n = d.n, m = n + 6, nh = halo_count(m);
-  const size_t fe = (size_t)6 * m * m, face = (size_t)6 * (n + 1) * n * 3;
+  // face cache blocks of the 8 x 16 tiles this entry point runs
+  const size_t fe = (size_t)6 * m * m,
+               face = (size_t)6 * ((n + 7) / 8) * ((n + 15) / 16) * TileShape<8, 16>::fW;
   const size_t o_src = kStatusBytes;
   const size_t o_w = o_src + align256((size_t)6 * nh * sizeof(int2));
   const size_t o_f = o_w + align256((size_t)6 * nh * 2 * sizeof(T));
   const int nfields = rk == 2 ? 3 : 6;
   const size_t o_fx = o_f + align256((size_t)nfields * fe * sizeof(T));
-  const size_t o_fy = o_fx + align256(face * sizeof(T));
-  const size_t need = o_fy + align256(face * sizeof(T));
+  const size_t need = o_fx + align256(face * sizeof(T));
   if (need > kScratchBytes)
     return set_error(BT_EINVAL, "bt_round_noalloc: N = " + std::to_string(n) + " needs " + std::to_string(need) +
                                     " bytes of scratch, more than the library's fixed " +
@@ -277,7 +277,6 @@ int run_noalloc(unsigned char* base, const bt_grid_desc& d, const bt_state_in& i
   T* hw = (T*)(base + o_w);
   T* F = (T*)(base + o_f);
   T* fx = (T*)(base + o_fx);
-  T* fy = (T*)(base + o_fy);
   const RouteTable rt = make_routes();
   const int cells = 6 * nh, th = 256;
   k_build_halo<T><<<(cells + th - 1) / th, th, 0, s>>>(n, (const T*)d.k2e_coef, d.loc_i_local, d.loc_j_local, rt,
@@ -320,17 +319,17 @@ int run_noalloc(unsigned char* base, const bt_grid_desc& d, const bt_state_in& i
     const T* const* bs = step == 0 ? B0 : (const T* const*)X;
     const int stored = step == 0 ? 1 : 0;
     if (rk == 2) {
-      e = stage(io_of<T>(cur[0], cur[1], cur[2], bs[0], bs[1], bs[2], Y[0], Y[1], Y[2], fx, fy, dtb / 2.0, 0.0,
+      e = stage(io_of<T>(cur[0], cur[1], cur[2], bs[0], bs[1], bs[2], Y[0], Y[1], Y[2], fx, dtb / 2.0, 0.0,
                          stored, 0));
       if (e == cudaSuccess)
-        e = stage(io_of<T>(Y[0], Y[1], Y[2], bs[0], bs[1], bs[2], X[0], X[1], X[2], fx, fy, dtb, 0.0, 0, 1));
+        e = stage(io_of<T>(Y[0], Y[1], Y[2], bs[0], bs[1], bs[2], X[0], X[1], X[2], fx, dtb, 0.0, 0, 1));
     } else {
-      e = stage(io_of<T>(cur[0], cur[1], cur[2], bs[0], bs[1], bs[2], Y[0], Y[1], Y[2], fx, fy, dtb / 3.0, 1.0,
+      e = stage(io_of<T>(cur[0], cur[1], cur[2], bs[0], bs[1], bs[2], Y[0], Y[1], Y[2], fx, dtb / 3.0, 1.0,
                          stored, 0));
       if (e == cudaSuccess)
-        e = stage(io_of<T>(Y[0], Y[1], Y[2], bs[0], bs[1], bs[2], Z[0], Z[1], Z[2], fx, fy, dtb / 2.0, 1.0, 0, 0));
+        e = stage(io_of<T>(Y[0], Y[1], Y[2], bs[0], bs[1], bs[2], Z[0], Z[1], Z[2], fx, dtb / 2.0, 1.0, 0, 0));
       if (e == cudaSuccess)
-        e = stage(io_of<T>(Z[0], Z[1], Z[2], bs[0], bs[1], bs[2], X[0], X[1], X[2], fx, fy, dtb, 1.0, 0, 1));
+        e = stage(io_of<T>(Z[0], Z[1], Z[2], bs[0], bs[1], bs[2], X[0], X[1], X[2], fx, dtb, 1.0, 0, 1));
     }
   }
   if (e == cudaSuccess && out.diag[0]) {

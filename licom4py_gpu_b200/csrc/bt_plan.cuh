@@ -79,13 +79,13 @@ struct bt_plan {
   }
 
   size_t esize() const { return dtype == BT_F64 ? 8 : 4; }
-  // scratch layout: 6 stage fields, edge lines (24 n), face caches x and y (6 (n+1) n 3 each)
-  size_t face_elems() const { return (size_t)6 * (n + 1) * n * 3; }
-  size_t scratch_elems() const { return 6 * field_elems + 24 * (size_t)n + 2 * face_elems(); }
+  // scratch layout: 6 stage fields, edge lines (24 n), then on a 256-byte boundary (16-byte copies)
+  // the face cache blocks, sized for every tile shape
+  size_t face_offset() const { return ((6 * field_elems + 24 * (size_t)n) * esize() + 255) & ~(size_t)255; }
+  size_t scratch_bytes() const { return face_offset() + face_cache_elems(n) * esize(); }
   void* scratch_field(int k) const { return (char*)scratch + (size_t)k * field_elems * esize(); }
   void* edge_lines() const { return scratch_field(6); }
-  void* face_x() const { return (char*)edge_lines() + 24 * (size_t)n * esize(); }
-  void* face_y() const { return (char*)face_x() + face_elems() * esize(); }
+  void* face_x() const { return (char*)scratch + face_offset(); }
 
   template <typename T>
   Geo<T> geo() const {

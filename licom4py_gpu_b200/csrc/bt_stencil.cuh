@@ -234,6 +234,9 @@ struct TileShape {
   static constexpr int FY = TI * (TJ + 1);          // y faces (r * (TJ + 1) + q)
   static constexpr int C = TI * TJ;                 // cells (a * TJ + q)
   static constexpr int EW = TI > TJ ? TI : TJ;
+  // face cache block of a tile (words): the three x-face planes [3][FX], then the three y-face planes
+  // [3][FY], each part padded to 16 bytes (four words)
+  static constexpr int fXB = (3 * FX + 3) & ~3, fYB = (3 * FY + 3) & ~3, fW = fXB + fYB;
   static constexpr int NE = 4 * EW;                 // edge slots: 4 kinds x max(TI, TJ) positions
   static constexpr int KV = (RI + NS - 1) / NS;     // row iterations over the vertical bar
   static constexpr int KX = (TI + 1 + NS - 1) / NS; // over x-face rows
@@ -342,10 +345,17 @@ __device__ __forceinline__ int cell32(int f, int i, int j, int m) { return (f * 
 // row fewer, so the extra column evens out the face work across the warps.
 __device__ __forceinline__ int east_row() { return (int)threadIdx.x - (kTileThreads - 32); }
 
-// Face-cache entries: x face (f, i', j') at (f (n + 1) + i') n + j', y face at
-// (f n + i') (n + 1) + j'; the three cached values sit in planes 6 (n + 1) n apart.
-__device__ __forceinline__ int xface_idx(int f, int ip, int jp, int n) { return (f * (n + 1) + ip) * n + jp; }
-__device__ __forceinline__ int yface_idx(int f, int ip, int jp, int n) { return (f * n + ip) * (n + 1) + jp; }
+// Offset of a tile's face cache block (TileShape::fW words per tile, tiles in
+// face-major, row-major order).  Each tile writes every face it computes into
+// its own block (the faces it shares with the next tile are computed by both,
+// identically), so phase UV of a tile reads only its own block: one
+// contiguous range, loaded with 16-byte copies.
+template <int TI, int TJ>
+__device__ __forceinline__ long face_block_off(const TileBox& b, int n) {
+  const int nti = (n + TI - 1) / TI, ntj = (n + TJ - 1) / TJ;
+  const int t = (b.f * nti + (b.i0 - kHalo) / TI) * ntj + (b.j0 - kHalo) / TJ;
+  return (long)t * TileShape<TI, TJ>::fW;
+}
 
 // ---- asynchronous global -> shared copies ---------------------------------
 template <int BYTES>
@@ -951,11 +961,10 @@ __device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, c
     const T nvis = bc + ncoef * (nhe - nhw);
     fl = (fl + (ndz * nvis + (nvis > T(0.0) ? nhe : nhw) * nvis)) / T(2.0);
   }
-  if (fc) {  // face cache for phase UV: three planes pstride apart
-    fc[0] = bc;
-    fc[pstride] = vis;
-    fc[2 * pstride] = T(0.5) * cc * (ue - uw);  // celerity viscosity flux, barotr_pure.py:68-69
-  }
+  // face cache for phase UV: three planes pstride apart
+  fc[0] = bc;
+  fc[pstride] = vis;
+  fc[2 * pstride] = T(0.5) * cc * (ue - uw);  // celerity viscosity flux, barotr_pure.py:68-69
   return fl;
 }
 
@@ -1070,8 +1079,9 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
   }
   __syncthreads();
 
-  // faces; their fluxes (times c_dy / d_dx) alias the metric block, no longer read
-  const int PF = 6 * (n + 1) * n;  // plane size of both face caches
+  // faces; their fluxes (times c_dy / d_dx) alias the metric block, no longer read.  The face
+  // cache of every face goes to the tile's block (phase UV's shared-memory layout when resident)
+  T* const fblk = RES ? nullptr : io.fx + face_block_off<TI, TJ>(b, n);
   if (q < nj) {
 #pragma unroll
     for (int k = 0; k < S::KX; ++k) {
@@ -1080,12 +1090,9 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
         const int side =
             FULL ? -1 : ((a == 0 && b.i0 == kHalo) ? kS : ((a == ni && b.i0 + ni == m - kHalo) ? kN : -1));
         const int e = a * TJ + q;
-        T* fc = RES ? U.s_xc + e
-                    : ((a < ni || side == kN) ? io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n)
-                                              : nullptr);
+        T* fc = RES ? U.s_xc + e : fblk + e;
         const T fl = face_h<T>(io, L.s_h + a * RJ + q + kHalo, RJ, L.s_uc + a * TJ + q, TJ, side,
-                               (side == kS ? 0 : 1) * S::EW + q, L.s_dzx[e], L.s_np, L.s_nh, L.s_ndz, fc,
-                               RES ? S::FX : PF);
+                               (side == kS ? 0 : 1) * S::EW + q, L.s_dzx[e], L.s_np, L.s_nh, L.s_ndz, fc, S::FX);
         L.s_P[e] = fl * L.s_cdy[e];
       }
     }
@@ -1106,12 +1113,9 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
     const int side =
         FULL ? -1 : ((qq == 0 && b.j0 == kHalo) ? kW : ((qq == nj && b.j0 + nj == m - kHalo) ? kE : -1));
     const int e = r * (TJ + 1) + qq;
-    T* fc = RES ? U.s_yc + e
-                : ((qq < nj || side == kE) ? io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n)
-                                           : nullptr);
+    T* fc = RES ? U.s_yc + e : fblk + S::fXB + e;
     const T fl = face_h<T>(io, L.s_h + (r + kHalo) * RJ + qq, 1, L.s_vc + r * RJ + qq, 1, side,
-                           (side == kW ? 2 : 3) * S::EW + r, L.s_dzy[e], L.s_np, L.s_nh, L.s_ndz, fc,
-                           RES ? S::FY : PF);
+                           (side == kW ? 2 : 3) * S::EW + r, L.s_dzy[e], L.s_np, L.s_nh, L.s_ndz, fc, S::FY);
     L.s_Q[e] = fl * L.s_ddx[e];
   }
   __syncthreads();
@@ -1197,42 +1201,17 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
   const LayoutUV<T, TI, TJ> L(sm);
   const bool blend = io.beta != T(0.0);  // fb_scheme needs the stage h only when beta_d != 0
   const T* hn_src = (const T*)io.h_out;
-  const int PF = 6 * (n + 1) * n;
   const T* const hb = RES ? rs.hs : L.s_hb;  // stage h of the blend, region layout [RI][RJ]
   const int* const items = RES ? rs.items : reinterpret_cast<const int*>(sm + S::kWordsUV);
 
-  // face caches of this stage (written by phase H) -> shared memory
-  if (!RES && q < nj) {
+  // the tile's face cache block of this stage (written by phase H) -> shared memory, 16 bytes a copy
+  if (!RES) {
+    constexpr int V = 16 / sizeof(T);
+    const T* blk = io.fx + face_block_off<TI, TJ>(b, n);
 #pragma unroll
-    for (int k = 0; k < S::KX; ++k) {
-      const int a = sl + k * S::NS;
-      if (a <= ni) {
-        const T* src = io.fx + xface_idx(f, b.i0 - kHalo + a, b.j0 - kHalo + q, n);
-        const int e = a * TJ + q;
-        cp_async_t(L.s_xc + e, src);
-        cp_async_t(L.s_xc + S::FX + e, src + PF);
-        cp_async_t(L.s_xc + 2 * S::FX + e, src + 2 * PF);
-      }
-    }
-  }
+    for (int w = threadIdx.x * V; w < S::fXB; w += kTileThreads * V) cp_async<16>(L.s_xc + w, blk + w);
 #pragma unroll
-  for (int k = 0; k <= S::KC; ++k) {
-    if (RES) break;
-    int r, qq;
-    if (k < S::KC) {
-      r = sl + k * S::NS;
-      qq = q;
-      if (r >= ni || q > nj) continue;
-    } else {
-      r = east_row();
-      qq = TJ;
-      if (nj != TJ || r < 0 || r >= ni) continue;
-    }
-    const T* src = io.fy + yface_idx(f, b.i0 - kHalo + r, b.j0 - kHalo + qq, n);
-    const int e = r * (TJ + 1) + qq;
-    cp_async_t(L.s_yc + e, src);
-    cp_async_t(L.s_yc + S::FY + e, src + PF);
-    cp_async_t(L.s_yc + 2 * S::FY + e, src + 2 * PF);
+    for (int w = threadIdx.x * V; w < S::fYB; w += kTileThreads * V) cp_async<16>(L.s_yc + w, blk + S::fXB + w);
   }
 
   // state of the region: interior points by cp.async straight into shared
@@ -1535,7 +1514,6 @@ __device__ __forceinline__ StageIO<T> round_stage(const RoundArgs<T>& a, int ste
   io.u_out = last ? a.x[1] : (st == 0 ? a.y[1] : a.z[1]);
   io.v_out = last ? a.x[2] : (st == 0 ? a.y[2] : a.z[2]);
   io.fx = a.fx;
-  io.fy = a.fy;
   double dt;
   if (a.rk == 2) {
     dt = st == 0 ? a.dtb / 2.0 : a.dtb;      // barotr.py:50-56
