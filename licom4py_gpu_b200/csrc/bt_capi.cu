@@ -282,6 +282,38 @@ cudaError_t enqueue_stage(const bt_plan* p, const bt_state_in& in, const bt_stat
   return launch_fill_halo<T>(g, X[0], X[1], X[2], s);
 }
 
+// Phase UV constant blocks for the plan's tile shape (Geo::uvb): built once,
+// stream-ordered on s, rebuilt after a tile change; without them (allocation
+// failure) phase UV reads the constant arrays as before.  Runs before any
+// capture of the round (bt_round builds them ahead of its graph).
+template <typename T>
+int ensure_uv_blocks(bt_plan* p, cudaStream_t s) {
+  if (p->d_uvb && p->uvb_tile.ti == p->tile.ti && p->uvb_tile.tj == p->tile.tj) return BT_OK;
+  const size_t bytes = uv_block_elems(p->tile, p->n) * sizeof(T);
+  if (bytes == 0) return BT_OK;
+  if (bytes > p->uvb_bytes) {
+    if (p->d_uvb) cudaFree(p->d_uvb);
+    p->d_uvb = nullptr;
+    p->uvb_bytes = 0;
+    if (cudaMalloc(&p->d_uvb, bytes) != cudaSuccess) {
+      cudaGetLastError();  // clear the allocation error: the arrays serve instead
+      p->d_uvb = nullptr;
+      return BT_OK;
+    }
+    p->uvb_bytes = bytes;
+  }
+  p->uvb_tile = {0, 0};
+  Geo<T> g = p->geo<T>();  // uvb not yet valid: the builder reads the arrays
+  const cudaError_t e = launch_uv_blocks<T>(g, p->tile, (T*)p->d_uvb, s);
+  if (e != cudaSuccess) return cuda_fail(e, "phase UV constant blocks");
+  p->uvb_tile = p->tile;
+  return BT_OK;
+}
+
+int ensure_uv_blocks_any(bt_plan* p, cudaStream_t s) {
+  return p->dtype == BT_F64 ? ensure_uv_blocks<double>(p, s) : ensure_uv_blocks<float>(p, s);
+}
+
 // Substeps per cooperative launch of the persistent and resident modes: a
 // round is split into launches of at most this many substeps, so the grid
 // barrier's 31-bit arrival count (2 x stages x substeps x CTAs) and the
@@ -607,6 +639,7 @@ int bt_plan_destroy(bt_plan* p) {
   if (p->d_hsrc) cudaFree(p->d_hsrc);
   if (p->d_hw) cudaFree(p->d_hw);
   if (p->d_res) cudaFree(p->d_res);
+  if (p->d_uvb) cudaFree(p->d_uvb);
   delete p;
   return BT_OK;
 }
@@ -647,6 +680,10 @@ int bt_round(bt_plan* p, const bt_state_in* in, const bt_state_out* out, int nbb
     for (int k = 1; k < 10; ++k)
       if (!out->diag[k]) return fail(BT_EINVAL, "bt_round: diag outputs must be all set or diag[0] NULL");
   cudaStream_t s = (cudaStream_t)stream;
+  {
+    const int rc = ensure_uv_blocks_any(p, s);
+    if (rc != BT_OK) return rc;
+  }
   if (p->mode == BT_MODE_RESIDENT)
     return p->dtype == BT_F64 ? enqueue_round_resident<double>(p, *in, *out, nbb, dtb, rk, s)
                               : enqueue_round_resident<float>(p, *in, *out, nbb, dtb, rk, s);
@@ -709,6 +746,10 @@ int bt_stage(bt_plan* p, const bt_state_in* in, const bt_state_out* out, double 
     for (int k = 1; k < 10; ++k)
       if (!out->diag[k]) return fail(BT_EINVAL, "bt_stage: diag outputs must be all set or diag[0] NULL");
   cudaStream_t s = (cudaStream_t)stream;
+  {
+    const int rc = ensure_uv_blocks_any(p, s);
+    if (rc != BT_OK) return rc;
+  }
   cudaError_t e = p->dtype == BT_F64 ? enqueue_stage<double>(p, *in, *out, dt, beta_d, is_laststep ? 1 : 0, s)
                                      : enqueue_stage<float>(p, *in, *out, dt, beta_d, is_laststep ? 1 : 0, s);
   if (e != cudaSuccess) return cuda_fail(e, "bt_stage: launch");

@@ -71,6 +71,11 @@ struct Geo {
   const T* d_dx;
   const int2* hsrc; // (6, nh) source offsets (absolute within the member)
   const T* hw;      // (6, nh, 2) interpolation weights
+  // Phase UV's constants of every tile, each block the image of its shared-memory
+  // constant area (TileShape::uG .. uCEnd), for tiles of uvb_ti x uvb_tj cells;
+  // nullptr, or another tile shape: the constants are read from the arrays above.
+  const T* uvb;
+  int uvb_ti, uvb_tj;
   int route[24];    // f*4 + side
 };
 

@@ -251,15 +251,17 @@ struct TileShape {
   static constexpr int hP = hG, hQ = hG + FX;
   static_assert(FX + FY <= 4 * NP, "face fluxes must fit in the metric block they alias");
   // phase UV (words): s_v [VB], s_u [TI][RJ], s_hn [RI][RJ], s_hb [RI][RJ] (stage h of
-  // the fb blend, RK3), cells g [C][4], sina,
-  // rda, rdx, rdy, a_f; x faces cache [3][FX], c_dy, kinetic energy, v_t * c_dy;
-  // y faces cache [3][FY], d_dx, kinetic energy, u_t * d_dx
+  // the fb blend, RK3); the constants, contiguous [uG, uCEnd): cells g [C][4], sina, rda,
+  // rdx, rdy, a_f, x faces c_dy, y faces d_dx; then x faces cache [3][FX], kinetic energy,
+  // v_t * c_dy; y faces cache [3][FY], kinetic energy, u_t * d_dx
   static constexpr int uV = 0, uU = up4(uV + VB), uHN = up4(uU + TI * RJ), uHB = up4(uHN + RI * RJ),
                        uG = up4(uHB + RI * RJ),
                        uSN = up4(uG + 4 * C), uRDA = uSN + C, uRDX = uRDA + C, uRDY = uRDX + C, uAF = uRDY + C,
-                       uXC = up4(uAF + C), uCDY = up4(uXC + 3 * FX), uKU = up4(uCDY + FX), uVX = up4(uKU + FX),
-                       uYC = up4(uVX + FX), uDDX = up4(uYC + 3 * FY), uKV = up4(uDDX + FY), uUY = up4(uKV + FY),
+                       uCDY = up4(uAF + C), uDDX = up4(uCDY + FX), uCEnd = up4(uDDX + FY),
+                       uXC = uCEnd, uKU = up4(uXC + 3 * FX), uVX = up4(uKU + FX),
+                       uYC = up4(uVX + FX), uKV = up4(uYC + 3 * FY), uUY = up4(uKV + FY),
                        kWordsUV = up4(uUY + FY);
+  static constexpr int uConstWords = uCEnd - uG;  // one tile's block of phase UV constants
 };
 
 struct TileBox {
@@ -351,10 +353,13 @@ __device__ __forceinline__ int east_row() { return (int)threadIdx.x - (kTileThre
 // identically), so phase UV of a tile reads only its own block: one
 // contiguous range, loaded with 16-byte copies.
 template <int TI, int TJ>
-__device__ __forceinline__ long face_block_off(const TileBox& b, int n) {
+__device__ __forceinline__ int tile_index(const TileBox& b, int n) {
   const int nti = (n + TI - 1) / TI, ntj = (n + TJ - 1) / TJ;
-  const int t = (b.f * nti + (b.i0 - kHalo) / TI) * ntj + (b.j0 - kHalo) / TJ;
-  return (long)t * TileShape<TI, TJ>::fW;
+  return (b.f * nti + (b.i0 - kHalo) / TI) * ntj + (b.j0 - kHalo) / TJ;
+}
+template <int TI, int TJ>
+__device__ __forceinline__ long face_block_off(const TileBox& b, int n) {
+  return (long)tile_index<TI, TJ>(b, n) * TileShape<TI, TJ>::fW;
 }
 
 // ---- asynchronous global -> shared copies ---------------------------------
@@ -1135,10 +1140,19 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
 }
 
 // ---- phase UV -----------------------------------------------------------------
-// Phase UV cell and face constants of the tile (cp.async, not yet awaited).
+// Phase UV cell and face constants of the tile (cp.async, not yet awaited):
+// the tile's prepared block with 16-byte copies when the plan has one for this
+// tile shape, else element by element from the constant arrays.
 template <typename T, int TI, int TJ, bool FULL>
 __device__ __forceinline__ void tile_uv_consts(const Geo<T>& g, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
+  if (g.uvb != nullptr && g.uvb_ti == TI && g.uvb_tj == TJ) {
+    constexpr int V = 16 / sizeof(T);
+    const T* blk = g.uvb + (long)tile_index<TI, TJ>(b, g.n) * S::uConstWords;
+#pragma unroll
+    for (int w = threadIdx.x * V; w < S::uConstWords; w += kTileThreads * V) cp_async<16>(sm + S::uG + w, blk + w);
+    return;
+  }
   const LayoutUV<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
   const int ni = FULL ? TI : b.ni, nj = FULL ? TJ : b.nj;
