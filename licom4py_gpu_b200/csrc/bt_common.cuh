@@ -71,11 +71,13 @@ struct Geo {
   const T* d_dx;
   const int2* hsrc; // (6, nh) source offsets (absolute within the member)
   const T* hw;      // (6, nh, 2) interpolation weights
-  // Phase UV's constants of every tile, each block the image of its shared-memory
-  // constant area (TileShape::uG .. uCEnd), for tiles of uvb_ti x uvb_tj cells;
-  // nullptr, or another tile shape: the constants are read from the arrays above.
-  const T* uvb;
-  int uvb_ti, uvb_tj;
+  // Tile constant blocks for tiles of cblk_ti x cblk_tj cells (TileShape::cW words
+  // per tile): the image of phase UV's shared-memory constant area
+  // (TileShape::uG .. uCEnd), then the depths of the tile's x and y faces; phase
+  // H of full interior tiles assembles its constants from its own block and its
+  // four neighbours'.  nullptr, or another tile shape: the arrays above are read.
+  const T* cblk;
+  int cblk_ti, cblk_tj;
   int route[24];    // f*4 + side
 };
 

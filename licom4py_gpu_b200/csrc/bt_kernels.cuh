@@ -96,20 +96,29 @@ __global__ void __launch_bounds__(kThreads, 3) k_round(RoundArgs<T> a) {
   }
 }
 
-// Phase UV constant blocks: word w of tile t's block is what tile_uv_consts
-// stages at shared-memory word uG + w for that tile (gct, sina, rda, rdx, rdy,
-// a_f of its cells, c_dy of its x faces, d_dx of its y faces); positions
-// outside a partial tile and the padding are zero.
+// Tile constant blocks: word w < uConstWords of tile t's block is what
+// tile_uv_consts stages at shared-memory word uG + w for that tile (gct, sina,
+// rda, rdx, rdy, a_f of its cells, c_dy of its x faces, d_dx of its y faces);
+// then dzph_x of its x faces and dzph_y of its y faces, indexed like phase H's
+// shared-memory planes.  Positions outside a partial tile and the padding are zero.
 template <typename T, int TI, int TJ>
-__global__ void __launch_bounds__(kThreads) k_uv_blocks(Geo<T> g, Tiling t, T* out) {
+__global__ void __launch_bounds__(kThreads) k_const_blocks(Geo<T> g, Tiling t, T* out) {
   using S = TileShape<TI, TJ>;
-  const long total = 6L * t.nti * t.ntj * S::uConstWords;
+  const long total = 6L * t.nti * t.ntj * S::cW;
   const int m = g.m;
   for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < total; k += (long)gridDim.x * blockDim.x) {
-    const int tile = (int)(k / S::uConstWords), o = S::uG + (int)(k - (long)tile * S::uConstWords);
+    const int tile = (int)(k / S::cW), w = (int)(k - (long)tile * S::cW), o = S::uG + w;
     const TileBox b = tile_box_at(t, g.n, tile);
     T v = T(0);
-    if (o < S::uSN) {
+    if (w >= S::bDZX) {
+      if (w < S::bDZY) {
+        const int e = w - S::bDZX, a = e / TJ, q = e % TJ;
+        if (a <= b.ni && q < b.nj) v = g.dzph_x[cell(b.f, b.i0 + a, b.j0 + q, m)];
+      } else if (w < S::bDZY + S::FY) {
+        const int e = w - S::bDZY, r = e / (TJ + 1), qq = e % (TJ + 1);
+        if (r < b.ni && qq <= b.nj) v = g.dzph_y[cell(b.f, b.i0 + r, b.j0 + qq, m)];
+      }
+    } else if (o < S::uSN) {
       const int e = (o - S::uG) / 4, comp = (o - S::uG) % 4, a = e / TJ, q = e % TJ;
       if (a < b.ni && q < b.nj) v = g.gct[4 * cell(b.f, b.i0 + a, b.j0 + q, m) + comp];
     } else if (o < S::uAF + S::C) {
@@ -164,19 +173,19 @@ size_t face_cache_elems_tile(int n) {
 
 namespace {
 template <int TI, int TJ>
-size_t uv_block_elems_tile(int n) {
+size_t const_block_elems_tile(int n) {
   const size_t nti = (n + TI - 1) / TI, ntj = (n + TJ - 1) / TJ;
-  return 6 * nti * ntj * (size_t)TileShape<TI, TJ>::uConstWords;
+  return 6 * nti * ntj * (size_t)TileShape<TI, TJ>::cW;
 }
 }  // namespace
 
-size_t uv_block_elems(TileCfg c, int n) {
-  if (c.ti == 7 && c.tj == 32) return uv_block_elems_tile<7, 32>(n);
-  if (c.ti == 8 && c.tj == 32) return uv_block_elems_tile<8, 32>(n);
-  if (c.ti == 15 && c.tj == 32) return uv_block_elems_tile<15, 32>(n);
-  if (c.ti == 16 && c.tj == 32) return uv_block_elems_tile<16, 32>(n);
-  if (c.ti == 8 && c.tj == 16) return uv_block_elems_tile<8, 16>(n);
-  if (c.ti == 16 && c.tj == 16) return uv_block_elems_tile<16, 16>(n);
+size_t const_block_elems(TileCfg c, int n) {
+  if (c.ti == 7 && c.tj == 32) return const_block_elems_tile<7, 32>(n);
+  if (c.ti == 8 && c.tj == 32) return const_block_elems_tile<8, 32>(n);
+  if (c.ti == 15 && c.tj == 32) return const_block_elems_tile<15, 32>(n);
+  if (c.ti == 16 && c.tj == 32) return const_block_elems_tile<16, 32>(n);
+  if (c.ti == 8 && c.tj == 16) return const_block_elems_tile<8, 16>(n);
+  if (c.ti == 16 && c.tj == 16) return const_block_elems_tile<16, 16>(n);
   return 0;
 }
 
@@ -311,22 +320,22 @@ cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, 
 }
 
 template <typename T, int TI, int TJ>
-cudaError_t launch_uv_blocks_tile(const Geo<T>& g, T* out, cudaStream_t s) {
+cudaError_t launch_const_blocks_tile(const Geo<T>& g, T* out, cudaStream_t s) {
   const Tiling t = make_tiling({TI, TJ}, g.n);
-  const long total = 6L * t.nti * t.ntj * TileShape<TI, TJ>::uConstWords;
+  const long total = 6L * t.nti * t.ntj * TileShape<TI, TJ>::cW;
   const int grid = (int)std::min<long>((total + kThreads - 1) / kThreads, 148L * 16);
-  k_uv_blocks<T, TI, TJ><<<grid, kThreads, 0, s>>>(g, t, out);
+  k_const_blocks<T, TI, TJ><<<grid, kThreads, 0, s>>>(g, t, out);
   return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_uv_blocks(const Geo<T>& g, TileCfg c, T* out, cudaStream_t s) {
-  if (c.ti == 7 && c.tj == 32) return launch_uv_blocks_tile<T, 7, 32>(g, out, s);
-  if (c.ti == 8 && c.tj == 32) return launch_uv_blocks_tile<T, 8, 32>(g, out, s);
-  if (c.ti == 15 && c.tj == 32) return launch_uv_blocks_tile<T, 15, 32>(g, out, s);
-  if (c.ti == 16 && c.tj == 32) return launch_uv_blocks_tile<T, 16, 32>(g, out, s);
-  if (c.ti == 8 && c.tj == 16) return launch_uv_blocks_tile<T, 8, 16>(g, out, s);
-  if (c.ti == 16 && c.tj == 16) return launch_uv_blocks_tile<T, 16, 16>(g, out, s);
+cudaError_t launch_const_blocks(const Geo<T>& g, TileCfg c, T* out, cudaStream_t s) {
+  if (c.ti == 7 && c.tj == 32) return launch_const_blocks_tile<T, 7, 32>(g, out, s);
+  if (c.ti == 8 && c.tj == 32) return launch_const_blocks_tile<T, 8, 32>(g, out, s);
+  if (c.ti == 15 && c.tj == 32) return launch_const_blocks_tile<T, 15, 32>(g, out, s);
+  if (c.ti == 16 && c.tj == 32) return launch_const_blocks_tile<T, 16, 32>(g, out, s);
+  if (c.ti == 8 && c.tj == 16) return launch_const_blocks_tile<T, 8, 16>(g, out, s);
+  if (c.ti == 16 && c.tj == 16) return launch_const_blocks_tile<T, 16, 16>(g, out, s);
   return cudaErrorInvalidValue;
 }
 
@@ -350,7 +359,7 @@ cudaError_t launch_diag(const Geo<T>& g, const T* h, const T* u, const T* v, con
   template cudaError_t launch_phase_h<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t);  \
   template cudaError_t launch_phase_uv<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t); \
   template cudaError_t launch_fill_halo<T>(const Geo<T>&, T*, T*, T*, cudaStream_t);                \
-  template cudaError_t launch_uv_blocks<T>(const Geo<T>&, TileCfg, T*, cudaStream_t);               \
+  template cudaError_t launch_const_blocks<T>(const Geo<T>&, TileCfg, T*, cudaStream_t);               \
   template cudaError_t launch_round<T>(const RoundArgs<T>&, TileCfg, int, cudaStream_t, int*);      \
   template cudaError_t launch_diag<T>(const Geo<T>&, const T*, const T*, const T*, const DiagOut<T>&, \
                                       cudaStream_t);

@@ -17,11 +17,11 @@ struct TileCfg {
 
 // Tile shapes compiled into the library (rows x columns of interior cells).
 bool tile_cfg_supported(TileCfg c);
-// Phase UV constant blocks (Geo::uvb) for tile shape c: elements needed, and a
+// Tile constant blocks (Geo::cblk) for tile shape c: elements needed, and a
 // stream-ordered build from the constant arrays of g.
-size_t uv_block_elems(TileCfg c, int n);
+size_t const_block_elems(TileCfg c, int n);
 template <typename T>
-cudaError_t launch_uv_blocks(const Geo<T>& g, TileCfg c, T* out, cudaStream_t s);
+cudaError_t launch_const_blocks(const Geo<T>& g, TileCfg c, T* out, cudaStream_t s);
 // Elements of the face cache blocks of one member at n cells per face edge,
 // enough for every supported tile shape (the plan's tile can change later).
 size_t face_cache_elems(int n);

@@ -302,8 +302,8 @@ int run_noalloc(unsigned char* base, const bt_grid_desc& d, const bt_state_in& i
   g.d_dx = (const T*)d.d_dx;
   g.hsrc = hsrc;
   g.hw = hw;
-  g.uvb = nullptr;  // no prepared constant blocks: phase UV reads the constant arrays
-  g.uvb_ti = g.uvb_tj = 0;
+  g.cblk = nullptr;  // no prepared constant blocks: phase UV reads the constant arrays
+  g.cblk_ti = g.cblk_tj = 0;
   for (int k = 0; k < 24; ++k) g.route[k] = rt.r[k];
 
   T* Y[3] = {F, F + fe, F + 2 * fe};

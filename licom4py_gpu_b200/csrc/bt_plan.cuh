@@ -39,10 +39,10 @@ struct bt_plan {
   // graph cache
   cudaGraphExec_t gexec = nullptr;
   std::vector<uintptr_t> gkey;
-  // phase UV constant blocks for tile shape uvb_tile (built on first use, see ensure_uv_blocks)
-  void* d_uvb = nullptr;
-  size_t uvb_bytes = 0;
-  TileCfg uvb_tile{0, 0};
+  // tile constant blocks for tile shape cblk_tile (built on first use, see ensure_const_blocks)
+  void* d_cblk = nullptr;
+  size_t cblk_bytes = 0;
+  TileCfg cblk_tile{0, 0};
   // host copy of the halo gather sources (the resident mode's dependency lists are built from it)
   std::vector<int2> h_src;
   // resident mode: dependency lists and progress flags of the tile shape res_tile, one device block:
@@ -111,10 +111,10 @@ struct bt_plan {
     g.d_dx = (const T*)c[16];
     g.hsrc = (const int2*)d_hsrc;
     g.hw = (const T*)d_hw;
-    const bool uvb_ok = d_uvb && uvb_tile.ti == tile.ti && uvb_tile.tj == tile.tj;
-    g.uvb = uvb_ok ? (const T*)d_uvb : nullptr;
-    g.uvb_ti = uvb_ok ? uvb_tile.ti : 0;
-    g.uvb_tj = uvb_ok ? uvb_tile.tj : 0;
+    const bool cblk_ok = d_cblk && cblk_tile.ti == tile.ti && cblk_tile.tj == tile.tj;
+    g.cblk = cblk_ok ? (const T*)d_cblk : nullptr;
+    g.cblk_ti = cblk_ok ? cblk_tile.ti : 0;
+    g.cblk_tj = cblk_ok ? cblk_tile.tj : 0;
     std::memcpy(g.route, route, sizeof(route));
     return g;
   }

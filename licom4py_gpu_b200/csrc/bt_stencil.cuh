@@ -261,7 +261,11 @@ struct TileShape {
                        uXC = uCEnd, uKU = up4(uXC + 3 * FX), uVX = up4(uKU + FX),
                        uYC = up4(uVX + FX), uKV = up4(uYC + 3 * FY), uUY = up4(uKV + FY),
                        kWordsUV = up4(uUY + FY);
-  static constexpr int uConstWords = uCEnd - uG;  // one tile's block of phase UV constants
+  static constexpr int uConstWords = uCEnd - uG;  // phase UV's constants of one tile
+  // tile constant block (words): phase UV's constant area image, then dzph_x of the x faces [FX]
+  // and dzph_y of the y faces [FY] (padded); plane offsets within the block
+  static constexpr int bSN = uSN - uG, bRDA = uRDA - uG, bCDY = uCDY - uG, bDDX = uDDX - uG,
+                       bDZX = uConstWords, bDZY = bDZX + FX, cW = bDZY + ((FY + 3) & ~3);
 };
 
 struct TileBox {
@@ -850,10 +854,58 @@ struct LayoutUV {
   }
 };
 
+// 16-byte copies of ``words`` words (a multiple of 16 bytes) from global src to shared dst.
+template <typename T, int WORDS>
+__device__ __forceinline__ void cp_async_run(T* dst, const T* src) {
+  constexpr int V = 16 / sizeof(T);
+  static_assert(WORDS % V == 0, "runs of whole 16-byte chunks");
+#pragma unroll
+  for (int w = threadIdx.x * V; w < WORDS; w += kTileThreads * V) cp_async<16>(dst + w, src + w);
+}
+
+// Phase H constants of a full interior tile from the tile constant blocks: the
+// region metric (vertical bar: 3 rows of the tile above, the tile's own rows, 3
+// rows of the tile below; side points: 3 columns of the tiles left and right --
+// all four exist on the same face for a full tile and hold at least 3 rows /
+// columns) and the tile's own face and cell constants, in 16-byte copies.
+template <typename T, int TI, int TJ>
+__device__ __forceinline__ void tile_h_consts_blocks(const Geo<T>& g, const TileBox& b, T* sm) {
+  using S = TileShape<TI, TJ>;
+  const LayoutH<T, TI, TJ> L(sm);
+  const int ntj = (g.n + TJ - 1) / TJ;
+  const T* own = g.cblk + (long)tile_index<TI, TJ>(b, g.n) * S::cW;
+  const T* above = own - (long)ntj * S::cW;
+  const T* below = own + (long)ntj * S::cW;
+  const T* left = own - S::cW;
+  const T* right = own + S::cW;
+  cp_async_run<T, 4 * 3 * TJ>(L.s_g, above + 4 * (TI - 3) * TJ);
+  cp_async_run<T, 4 * TI * TJ>(L.s_g + 4 * 3 * TJ, own);
+  cp_async_run<T, 4 * 3 * TJ>(L.s_g + 4 * (TI + 3) * TJ, below);
+  cp_async_run<T, 3 * TJ>(L.s_sn, above + S::bSN + (TI - 3) * TJ);
+  cp_async_run<T, TI * TJ>(L.s_sn + 3 * TJ, own + S::bSN);
+  cp_async_run<T, 3 * TJ>(L.s_sn + (TI + 3) * TJ, below + S::bSN);
+  if (threadIdx.x < 6 * TI) {  // side point (r, c): columns TJ-3.. of the left tile, 0..2 of the right one
+    const int t = threadIdx.x, r = t / 6, c = t - 6 * r;
+    const T* nb = c < 3 ? left : right;
+    const int e = c < 3 ? r * TJ + TJ - 3 + c : r * TJ + c - 3;  // the cell within the neighbour's block
+    cp_async_mat(L.s_g + 4 * (S::VB + t), nb + 4 * e);            // metric plane first, 4 words per cell
+    cp_async_t(L.s_sn + S::VB + t, nb + S::bSN + e);
+  }
+  cp_async_run<T, S::C>(L.s_rda, own + S::bRDA);
+  cp_async_run<T, S::FX>(L.s_cdy, own + S::bCDY);
+  cp_async_run<T, S::FX>(L.s_dzx, own + S::bDZX);
+  cp_async_run<T, (S::FY + 3) & ~3>(L.s_ddx, own + S::bDDX);
+  cp_async_run<T, (S::FY + 3) & ~3>(L.s_dzy, own + S::bDZY);
+}
+
 // Phase H constants of the tile (cp.async, not yet awaited).
 template <typename T, int TI, int TJ, bool FULL>
 __device__ __forceinline__ void tile_h_consts(const Geo<T>& g, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
+  if (FULL && g.cblk != nullptr && g.cblk_ti == TI && g.cblk_tj == TJ) {
+    tile_h_consts_blocks<T, TI, TJ>(g, b, sm);
+    return;
+  }
   const LayoutH<T, TI, TJ> L(sm);
   const int m = g.m, q = threadIdx.x % TJ, sl = threadIdx.x / TJ;
   const int ni = FULL ? TI : b.ni, nj = FULL ? TJ : b.nj;
@@ -1146,9 +1198,9 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
 template <typename T, int TI, int TJ, bool FULL>
 __device__ __forceinline__ void tile_uv_consts(const Geo<T>& g, const TileBox& b, T* sm) {
   using S = TileShape<TI, TJ>;
-  if (g.uvb != nullptr && g.uvb_ti == TI && g.uvb_tj == TJ) {
+  if (g.cblk != nullptr && g.cblk_ti == TI && g.cblk_tj == TJ) {
     constexpr int V = 16 / sizeof(T);
-    const T* blk = g.uvb + (long)tile_index<TI, TJ>(b, g.n) * S::uConstWords;
+    const T* blk = g.cblk + (long)tile_index<TI, TJ>(b, g.n) * S::cW;
 #pragma unroll
     for (int w = threadIdx.x * V; w < S::uConstWords; w += kTileThreads * V) cp_async<16>(sm + S::uG + w, blk + w);
     return;
