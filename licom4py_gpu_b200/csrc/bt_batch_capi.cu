@@ -94,7 +94,10 @@ int batch_round(bt_batch* b, const bt_member* mem, int count, int rk, cudaStream
     if (gi == (int)plans.size()) {
       if (gi == kMaxGeo) return bfail(BT_EINVAL, "bt_batch_round: more than 16 distinct plans in one call");
       plans.push_back(p);
-      hg[gi] = p->geo<T>();
+      // the member plan's constant blocks for the batch's tile shape, built once per plan
+      const int rc = ensure_const_blocks_any(u.plan, b->tile, s);
+      if (rc != BT_OK) return rc;
+      hg[gi] = p->geo_tile<T>(b->tile);
     }
     const ScratchLayout L = scratch_layout(p, rk);
     char* sc = (char*)u.scratch;

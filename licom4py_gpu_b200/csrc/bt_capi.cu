@@ -282,37 +282,45 @@ cudaError_t enqueue_stage(const bt_plan* p, const bt_state_in& in, const bt_stat
   return launch_fill_halo<T>(g, X[0], X[1], X[2], s);
 }
 
-// Tile constant blocks for the plan's tile shape (Geo::cblk): built once,
-// stream-ordered on s, rebuilt after a tile change; without them (allocation
+}  // namespace
+
+namespace bt {
+// Tile constant blocks of plan p for tile shape t (Geo::cblk): built once per
+// shape into a buffer of their own on stream s, which is then synchronised, so
+// rounds on any stream may use them afterwards; without them (allocation
 // failure) the phases read the constant arrays as before.  Runs before any
-// capture of the round (bt_round builds them ahead of its graph).
+// capture of the round (bt_round builds them ahead of its graph), so the
+// first round of a plan per tile shape must not be inside a stream capture.
 template <typename T>
-int ensure_const_blocks(bt_plan* p, cudaStream_t s) {
-  if (p->d_cblk && p->cblk_tile.ti == p->tile.ti && p->cblk_tile.tj == p->tile.tj) return BT_OK;
-  const size_t bytes = const_block_elems(p->tile, p->n) * sizeof(T);
-  if (bytes == 0) return BT_OK;
-  if (bytes > p->cblk_bytes) {
-    if (p->d_cblk) cudaFree(p->d_cblk);
-    p->d_cblk = nullptr;
-    p->cblk_bytes = 0;
-    if (cudaMalloc(&p->d_cblk, bytes) != cudaSuccess) {
-      cudaGetLastError();  // clear the allocation error: the arrays serve instead
-      p->d_cblk = nullptr;
-      return BT_OK;
-    }
-    p->cblk_bytes = bytes;
+int ensure_const_blocks(bt_plan* p, TileCfg t, cudaStream_t s) {
+  if (p->cblk_for(t)) return BT_OK;
+  const size_t bytes = const_block_elems(t, p->n) * sizeof(T);
+  bt_plan::ConstBlocks* slot = nullptr;
+  for (bt_plan::ConstBlocks& c : p->cblks)
+    if (!c.ptr) slot = &c;
+  if (bytes == 0 || !slot) return BT_OK;
+  if (cudaMalloc(&slot->ptr, bytes) != cudaSuccess) {
+    cudaGetLastError();  // clear the allocation error: the arrays serve instead
+    slot->ptr = nullptr;
+    return BT_OK;
   }
-  p->cblk_tile = {0, 0};
-  Geo<T> g = p->geo<T>();  // no valid blocks yet: the builder reads the arrays
-  const cudaError_t e = launch_const_blocks<T>(g, p->tile, (T*)p->d_cblk, s);
-  if (e != cudaSuccess) return cuda_fail(e, "phase UV constant blocks");
-  p->cblk_tile = p->tile;
+  cudaError_t e = launch_const_blocks<T>(p->geo_arrays<T>(), t, (T*)slot->ptr, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cudaFree(slot->ptr);
+    slot->ptr = nullptr;
+    return set_error(BT_ECUDA, std::string("tile constant blocks: ") + cudaGetErrorString(e));
+  }
+  slot->tile = t;
   return BT_OK;
 }
 
-int ensure_const_blocks_any(bt_plan* p, cudaStream_t s) {
-  return p->dtype == BT_F64 ? ensure_const_blocks<double>(p, s) : ensure_const_blocks<float>(p, s);
+int ensure_const_blocks_any(bt_plan* p, TileCfg t, cudaStream_t s) {
+  return p->dtype == BT_F64 ? ensure_const_blocks<double>(p, t, s) : ensure_const_blocks<float>(p, t, s);
 }
+}  // namespace bt
+
+namespace {
 
 // Substeps per cooperative launch of the persistent and resident modes: a
 // round is split into launches of at most this many substeps, so the grid
@@ -639,7 +647,8 @@ int bt_plan_destroy(bt_plan* p) {
   if (p->d_hsrc) cudaFree(p->d_hsrc);
   if (p->d_hw) cudaFree(p->d_hw);
   if (p->d_res) cudaFree(p->d_res);
-  if (p->d_cblk) cudaFree(p->d_cblk);
+  for (bt_plan::ConstBlocks& c : p->cblks)
+    if (c.ptr) cudaFree(c.ptr);
   delete p;
   return BT_OK;
 }
@@ -681,7 +690,7 @@ int bt_round(bt_plan* p, const bt_state_in* in, const bt_state_out* out, int nbb
       if (!out->diag[k]) return fail(BT_EINVAL, "bt_round: diag outputs must be all set or diag[0] NULL");
   cudaStream_t s = (cudaStream_t)stream;
   {
-    const int rc = ensure_const_blocks_any(p, s);
+    const int rc = ensure_const_blocks_any(p, p->tile, s);
     if (rc != BT_OK) return rc;
   }
   if (p->mode == BT_MODE_RESIDENT)
@@ -747,7 +756,7 @@ int bt_stage(bt_plan* p, const bt_state_in* in, const bt_state_out* out, double 
       if (!out->diag[k]) return fail(BT_EINVAL, "bt_stage: diag outputs must be all set or diag[0] NULL");
   cudaStream_t s = (cudaStream_t)stream;
   {
-    const int rc = ensure_const_blocks_any(p, s);
+    const int rc = ensure_const_blocks_any(p, p->tile, s);
     if (rc != BT_OK) return rc;
   }
   cudaError_t e = p->dtype == BT_F64 ? enqueue_stage<double>(p, *in, *out, dt, beta_d, is_laststep ? 1 : 0, s)

@@ -24,6 +24,12 @@ inline bool matrices_aligned(const bt_grid_desc* d) {
   return (((uintptr_t)d->a_c2l | (uintptr_t)d->a_l2c | (uintptr_t)d->a_gct) & 15) == 0;
 }
 
+struct bt_plan;
+namespace bt {
+// Build the tile constant blocks of plan p for tile shape t if it has none (bt_capi.cu).
+int ensure_const_blocks_any(bt_plan* p, TileCfg t, cudaStream_t s);
+}  // namespace bt
+
 struct bt_plan {
   int n = 0, m = 0, nh = 0, dtype = BT_F64, device = 0;
   TileCfg tile{8, 32};
@@ -39,10 +45,18 @@ struct bt_plan {
   // graph cache
   cudaGraphExec_t gexec = nullptr;
   std::vector<uintptr_t> gkey;
-  // tile constant blocks for tile shape cblk_tile (built on first use, see ensure_const_blocks)
-  void* d_cblk = nullptr;
-  size_t cblk_bytes = 0;
-  TileCfg cblk_tile{0, 0};
+  // tile constant blocks, one buffer per tile shape used (built on first use, see ensure_const_blocks):
+  // the plan's own rounds use the plan's tile, batched rounds the batch's
+  struct ConstBlocks {
+    TileCfg tile{0, 0};
+    void* ptr = nullptr;
+  };
+  ConstBlocks cblks[6];
+  const ConstBlocks* cblk_for(TileCfg t) const {
+    for (const ConstBlocks& c : cblks)
+      if (c.ptr && c.tile.ti == t.ti && c.tile.tj == t.tj) return &c;
+    return nullptr;
+  }
   // host copy of the halo gather sources (the resident mode's dependency lists are built from it)
   std::vector<int2> h_src;
   // resident mode: dependency lists and progress flags of the tile shape res_tile, one device block:
@@ -91,8 +105,23 @@ struct bt_plan {
   void* edge_lines() const { return scratch_field(6); }
   void* face_x() const { return (char*)scratch + face_offset(); }
 
+  // geometry for kernels of tile shape t (its constant blocks if built)
+  template <typename T>
+  Geo<T> geo_tile(TileCfg t) const {
+    Geo<T> g = geo_arrays<T>();
+    const ConstBlocks* c = cblk_for(t);
+    g.cblk = c ? (const T*)c->ptr : nullptr;
+    g.cblk_ti = c ? t.ti : 0;
+    g.cblk_tj = c ? t.tj : 0;
+    return g;
+  }
   template <typename T>
   Geo<T> geo() const {
+    return geo_tile<T>(tile);
+  }
+  // geometry without constant blocks (the arrays only)
+  template <typename T>
+  Geo<T> geo_arrays() const {
     Geo<T> g;
     g.n = n;
     g.m = m;
@@ -111,10 +140,8 @@ struct bt_plan {
     g.d_dx = (const T*)c[16];
     g.hsrc = (const int2*)d_hsrc;
     g.hw = (const T*)d_hw;
-    const bool cblk_ok = d_cblk && cblk_tile.ti == tile.ti && cblk_tile.tj == tile.tj;
-    g.cblk = cblk_ok ? (const T*)d_cblk : nullptr;
-    g.cblk_ti = cblk_ok ? cblk_tile.ti : 0;
-    g.cblk_tj = cblk_ok ? cblk_tile.tj : 0;
+    g.cblk = nullptr;
+    g.cblk_ti = g.cblk_tj = 0;
     std::memcpy(g.route, route, sizeof(route));
     return g;
   }
