@@ -262,8 +262,7 @@ namespace {
 
 template <typename T, int TI, int TJ, bool UV>
 size_t batch_tile_smem() {
-  using S = TileShape<TI, TJ>;
-  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH) + sizeof(int) * kItemWords;
+  return phase_smem_bytes<T, TI, TJ, UV>();
 }
 
 template <typename T, int TI, int TJ>

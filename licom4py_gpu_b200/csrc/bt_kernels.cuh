@@ -210,8 +210,7 @@ namespace {
 
 template <typename T, int TI, int TJ, bool UV>
 size_t tile_smem() {
-  using S = TileShape<TI, TJ>;
-  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH) + sizeof(int) * kItemWords;
+  return phase_smem_bytes<T, TI, TJ, UV>();
 }
 
 // The persistent kernel runs both phases in one allocation: the larger of the two.
