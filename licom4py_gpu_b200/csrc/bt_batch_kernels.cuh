@@ -262,7 +262,8 @@ namespace {
 
 template <typename T, int TI, int TJ, bool UV>
 size_t batch_tile_smem() {
-  return phase_smem_bytes<T, TI, TJ, UV>();
+  using S = TileShape<TI, TJ>;
+  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH) + sizeof(int) * kItemWords;
 }
 
 template <typename T, int TI, int TJ>

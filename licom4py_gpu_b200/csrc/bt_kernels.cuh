@@ -210,7 +210,8 @@ namespace {
 
 template <typename T, int TI, int TJ, bool UV>
 size_t tile_smem() {
-  return phase_smem_bytes<T, TI, TJ, UV>();
+  using S = TileShape<TI, TJ>;
+  return sizeof(T) * (UV ? S::kWordsUV : S::kWordsH) + sizeof(int) * kItemWords;
 }
 
 // The persistent kernel runs both phases in one allocation: the larger of the two.

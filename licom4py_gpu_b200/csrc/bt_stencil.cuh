@@ -508,28 +508,6 @@ struct ItemCell {
 // Only the writing thread reads them back (after the grid dependency), so the
 // decode's cold code stays off the critical path without holding registers.
 constexpr int kItemWords = 2 * kTileThreads;
-
-// The constants of each thread's first gather item (c2l at both sources, l2c,
-// the gct row and sina at the target, the face depth of a line's centre point)
-// are copied into per-thread shared-memory slots in the prologue, before the
-// grid dependency, for the 8 x 16 tiles of the small grids: their edge tiles
-// set the pace there, and these loads were a third of the edge tiles' staging
-// time.  kVals words per thread, value k of thread t at k * kTileThreads + t
-// (conflict-free reads), placed after the item words.
-template <typename T, int TI, int TJ>
-struct ItemPre {
-  static constexpr bool on = TI * TJ == 128;
-  static constexpr int kVals = 16;
-  static constexpr size_t bytes = on ? sizeof(T) * kVals * kTileThreads : 0;
-};
-
-// Dynamic shared memory of a tile phase: the phase's layout, the gather item
-// words and the items' constant slots.
-template <typename T, int TI, int TJ, bool UV>
-constexpr size_t phase_smem_bytes() {
-  return sizeof(T) * (UV ? TileShape<TI, TJ>::kWordsUV : TileShape<TI, TJ>::kWordsH) + sizeof(int) * kItemWords +
-         ItemPre<T, TI, TJ>::bytes;
-}
 __device__ __forceinline__ int pack_item(const ItemCell& c) {
   return c.r | (c.c << 6) | (c.slot << 12) | (c.line << 22) | (c.kind << 23) | (c.y << 25) | ((c.q == 3) << 26);
 }
@@ -626,7 +604,6 @@ struct Gather {
   // phase H gathers the region halo and the neighbour edge lines (9 items per
   // edge position); phase UV only the region halo (3 per position)
   static constexpr int kPerPos = UV ? 3 : 9;
-  static constexpr bool kPre = ItemPre<T, TI, TJ>::on && !RES;  // first item's constants pre-copied
   Pull<T> pd;  // descriptor of the thread's first item
   bool pl;
 
@@ -649,27 +626,6 @@ struct Gather {
         pd = pull_desc(g, c.f, c.i, c.j);
         pl = true;
       }
-      if constexpr (kPre) precopy(g, io, c, reinterpret_cast<T*>(s_items + kItemWords));
-    }
-  }
-
-  // The first item's constants into the thread's slots (cp.async, awaited in sources()).
-  __device__ __forceinline__ void precopy(const Geo<T>& g, const StageIO<T>& io, const ItemCell& c, T* s_pre) const {
-    const int t = threadIdx.x, o = c.o;
-    const bool vpull = UV ? !io.stored_halo : pl;
-    const int sa = vpull ? pd.s.x : o, sb = vpull ? pd.s.y : o;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      cp_async_t(s_pre + k * kTileThreads + t, g.c2l + 4 * (long)sa + k);
-      cp_async_t(s_pre + (4 + k) * kTileThreads + t, g.c2l + 4 * (long)sb + k);
-      cp_async_t(s_pre + (8 + k) * kTileThreads + t, g.l2c + 4 * (long)o + k);
-    }
-    if constexpr (!UV) {
-      const bool yaxis = c.line ? c.y : c.kind >= 2;
-      cp_async_t(s_pre + 12 * kTileThreads + t, g.gct + 4 * (long)o + (yaxis ? 2 : 0));
-      cp_async_t(s_pre + 13 * kTileThreads + t, g.gct + 4 * (long)o + (yaxis ? 3 : 1));
-      cp_async_t(s_pre + 14 * kTileThreads + t, g.sina + o);
-      if (c.line && io.last && c.q == 3) cp_async_t(s_pre + 15 * kTileThreads + t, (c.y ? g.dzph_y : g.dzph_x) + o);
     }
   }
 
@@ -679,7 +635,7 @@ struct Gather {
   // trip, not one per kind; the results are selected afterwards (a direct
   // read stays exact), and all loads precede the item's shared-memory stores.
   __device__ __forceinline__ void one(const Geo<T>& g, const StageIO<T>& io, const ItemCell& c, const Pull<T>& p,
-                                      bool pull, const GatherSink<T>& k, const T* pre = nullptr) {
+                                      bool pull, const GatherSink<T>& k) {
     if constexpr (UV && RES) {
       // resident phase UV: the raw velocities and the stage h of the halo
       // point were staged by phase H; only the new h is interpolated here
@@ -694,18 +650,9 @@ struct Gather {
     const int sa = vpull ? p.s.x : o, sb = vpull ? p.s.y : o;
     const T ua = io.u[sa], va = io.v[sa], ub = io.u[sb], vb = io.v[sb];
     T c0[4], c1[4], l2[4];
-    if (pre) {  // copied in the prologue (precopy)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        c0[q] = pre[q * kTileThreads + threadIdx.x];
-        c1[q] = pre[(4 + q) * kTileThreads + threadIdx.x];
-        l2[q] = pre[(8 + q) * kTileThreads + threadIdx.x];
-      }
-    } else {
-      ld_quad(g.c2l + 4 * (long)sa, c0);
-      ld_quad(g.c2l + 4 * (long)sb, c1);
-      ld_quad(g.l2c + 4 * (long)o, l2);
-    }
+    ld_quad(g.c2l + 4 * (long)sa, c0);
+    ld_quad(g.c2l + 4 * (long)sb, c1);
+    ld_quad(g.l2c + 4 * (long)o, l2);
     if (!UV) {
       const bool want_h = !c.line || io.last;  // region h, or the neighbour h of the mass-flux average
       T ha = T(0.0), hb = T(0.0), dz = T(0.0);
@@ -714,17 +661,10 @@ struct Gather {
         hb = io.h[sb];
       }
       const bool yaxis = c.line ? c.y : c.kind >= 2;  // contravariant component normal to the faces read
-      T g0, g1, sn;
-      if (pre) {
-        g0 = pre[12 * kTileThreads + threadIdx.x];
-        g1 = pre[13 * kTileThreads + threadIdx.x];
-        sn = pre[14 * kTileThreads + threadIdx.x];
-        if (c.line && want_h && c.q == 3) dz = pre[15 * kTileThreads + threadIdx.x];
-      } else {
-        ld_pair(g.gct + 4 * (long)o + (yaxis ? 2 : 0), g0, g1);
-        sn = g.sina[o];
-        if (c.line && want_h && c.q == 3) dz = (c.y ? g.dzph_y : g.dzph_x)[o];
-      }
+      T g0, g1;
+      ld_pair(g.gct + 4 * (long)o + (yaxis ? 2 : 0), g0, g1);
+      const T sn = g.sina[o];
+      if (c.line && want_h && c.q == 3) dz = (c.y ? g.dzph_y : g.dzph_x)[o];
       T u = ua, v = va, h = ha;
       if (vpull) {  // ext_vector / ext_scalar, cube.py:130-153
         const T ull0 = c0[0] * ua + c0[1] * va, vll0 = c0[2] * ua + c0[3] * va;
@@ -791,26 +731,19 @@ struct Gather {
   __device__ __forceinline__ void sources(const Geo<T>& g, const StageIO<T>& io, const TileBox& b,
                                           const EdgeCnt& cnt, int P, const GatherSink<T>& k, const int* s_items) {
     const int nitems = kPerPos * P;
-    const T* s_pre = nullptr;
-    if constexpr (kPre) {
-      cp_async_wait_all();  // this thread's own slots (and its prologue copies)
-      s_pre = reinterpret_cast<const T*>(s_items + kItemWords);
-    }
 #pragma unroll 1
     for (int t = threadIdx.x; t < nitems; t += kTileThreads) {
       bool pull = pl;
       Pull<T> p = pd;
       ItemCell c;
-      const T* pre = nullptr;
       if (t < kTileThreads) {
         c = unpack_item(s_items[t], s_items[kTileThreads + t]);
-        pre = s_pre;
       } else {
         c = decode_item(b, cnt, P, t, g.m, g.n, S::EW);
         pull = needs_pull(io, c, g.m);
         if (pull) p = pull_desc(g, c.f, c.i, c.j);
       }
-      one(g, io, c, p, pull, k, pre);
+      one(g, io, c, p, pull, k);
     }
   }
 };
