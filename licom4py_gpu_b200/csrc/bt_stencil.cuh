@@ -986,6 +986,35 @@ __device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& 
   tile_desc<T, TI, TJ, FULL, false, false>(g, io, b, gat, cnt, P, reinterpret_cast<int*>(sm + S::kWordsH));
 }
 
+// The neighbour's side of every edge face of a tile, from its gathered 6-point
+// lines (slot = edge kind x EW + position): its raw C-grid normal velocity
+// (line_raw) replaces the line's first velocity value and, on the last stage,
+// its reconstructed face h values and celerity viscosity coefficient replace
+// the line's first three h values.  Run between the staging barriers, one edge
+// position per thread counted from the CTA's last thread (the threads with the
+// fewest region points), so that the face pass of an edge face carries one
+// square root and division chain instead of two.
+template <typename T, int EW>
+__device__ __forceinline__ void edge_lines(const StageIO<T>& io, const TileBox& b, const EdgeCnt& cnt, int P, T* s_np,
+                                           T* s_nh, const T* s_ndz) {
+  for (int k = kTileThreads - 1 - (int)threadIdx.x; k < P; k += kTileThreads) {
+    const EdgeItem e = edge_item(b, cnt, k);
+    const int slot = e.kind * EW + e.pos;
+    T* np = s_np + 6 * slot;
+    const T lr = line_raw(np);
+    if (io.last) {
+      T* nh = s_nh + 6 * slot;
+      const T nhe = rplus(nh, 1), nhw = rminus(nh + 1, 1);
+      T nc, ncoef;
+      celerity_coef(mid6(nh, 1), s_ndz[slot], nc, ncoef);
+      nh[0] = nhe;
+      nh[1] = nhw;
+      nh[2] = ncoef;
+    }
+    np[0] = lr;
+  }
+}
+
 // Phase H of one x face or y face: C-grid normal velocity (remap.py:41-55)
 // and its edge average (communication.py:504-570), upwind mass flux with the
 // celerity-based velocity viscosity (barotr_pure.py:21-49) and its edge
@@ -1003,18 +1032,16 @@ __device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, c
   }
   const T ue = rplus(uu, 1), uw = rminus(uu + 1, 1);
   T bc = T(0.5) * (ue + uw);
-  if (side >= 0) bc = (bc + line_raw(s_np + 6 * slot)) / T(2.0);
+  if (side >= 0) bc = (bc + s_np[6 * slot]) / T(2.0);  // the neighbour's raw normal velocity (edge_lines)
   const T he = rplus(hh, 1), hw = rminus(hh + 1, 1);
   T cc, coef;
   celerity_coef(mid6(hh, 1), dz, cc, coef);
   const T vis = bc + coef * (he - hw);
   T fl = dz * vis + (vis > T(0.0) ? he : hw) * vis;
   if (io.last && side >= 0) {  // the neighbour's flux at the same edge face (barotr_pure.py:29-49)
-    const T* nh = s_nh + 6 * slot;
+    const T* nh = s_nh + 6 * slot;  // its face values and viscosity coefficient (edge_lines)
     const T ndz = s_ndz[slot];
-    const T nhe = rplus(nh, 1), nhw = rminus(nh + 1, 1);
-    T nc, ncoef;
-    celerity_coef(mid6(nh, 1), ndz, nc, ncoef);
+    const T nhe = nh[0], nhw = nh[1], ncoef = nh[2];
     const T nvis = bc + ncoef * (nhe - nhw);
     fl = (fl + (ndz * nvis + (nvis > T(0.0) ? nhe : nhw) * nvis)) / T(2.0);
   }
@@ -1134,6 +1161,7 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
     L.s_vc[sr * RJ + scc] = (G[2] * us + G[3] * vs) * sn;
     if constexpr (RES) U.s_u[sr * RJ + scc] = us;
   }
+  if (!FULL && P > 0) edge_lines<T, S::EW>(io, b, cnt, P, L.s_np, L.s_nh, L.s_ndz);
   __syncthreads();
 
   // faces; their fluxes (times c_dy / d_dx) alias the metric block, no longer read.  The face
