@@ -993,7 +993,14 @@ __device__ __forceinline__ void tile_h_pro_t(const Geo<T>& g, const StageIO<T>& 
 // the line's first three h values.  Run between the staging barriers, one edge
 // position per thread counted from the CTA's last thread (the threads with the
 // fewest region points), so that the face pass of an edge face carries one
-// square root and division chain instead of two.
+// square root and division chain instead of two.  float64 only: measured on a
+// B200 it shortens the float64 round (C96 16.60 -> 16.15 us per substep, C384
+// 160.3 -> 157.9) and lengthens the float32 one (C384 69.1 -> 70.7, C768
+// 293.5 -> 313.4), whose face chains are short and whose extra staging pass
+// costs more than it saves.
+template <typename T>
+__host__ __device__ constexpr bool edge_lines_staged() { return sizeof(T) == 8; }
+
 template <typename T, int EW>
 __device__ __forceinline__ void edge_lines(const StageIO<T>& io, const TileBox& b, const EdgeCnt& cnt, int P, T* s_np,
                                            T* s_nh, const T* s_ndz) {
@@ -1032,16 +1039,29 @@ __device__ __forceinline__ T face_h(const StageIO<T>& io, const T* ph, int sh, c
   }
   const T ue = rplus(uu, 1), uw = rminus(uu + 1, 1);
   T bc = T(0.5) * (ue + uw);
-  if (side >= 0) bc = (bc + s_np[6 * slot]) / T(2.0);  // the neighbour's raw normal velocity (edge_lines)
+  if (side >= 0) {  // the neighbour's raw normal velocity
+    const T nraw = edge_lines_staged<T>() ? s_np[6 * slot] : line_raw(s_np + 6 * slot);
+    bc = (bc + nraw) / T(2.0);
+  }
   const T he = rplus(hh, 1), hw = rminus(hh + 1, 1);
   T cc, coef;
   celerity_coef(mid6(hh, 1), dz, cc, coef);
   const T vis = bc + coef * (he - hw);
   T fl = dz * vis + (vis > T(0.0) ? he : hw) * vis;
   if (io.last && side >= 0) {  // the neighbour's flux at the same edge face (barotr_pure.py:29-49)
-    const T* nh = s_nh + 6 * slot;  // its face values and viscosity coefficient (edge_lines)
+    const T* nh = s_nh + 6 * slot;
     const T ndz = s_ndz[slot];
-    const T nhe = nh[0], nhw = nh[1], ncoef = nh[2];
+    T nhe, nhw, ncoef;
+    if constexpr (edge_lines_staged<T>()) {  // its face values and viscosity coefficient, staged
+      nhe = nh[0];
+      nhw = nh[1];
+      ncoef = nh[2];
+    } else {
+      nhe = rplus(nh, 1);
+      nhw = rminus(nh + 1, 1);
+      T nc;
+      celerity_coef(mid6(nh, 1), ndz, nc, ncoef);
+    }
     const T nvis = bc + ncoef * (nhe - nhw);
     fl = (fl + (ndz * nvis + (nvis > T(0.0) ? nhe : nhw) * nvis)) / T(2.0);
   }
@@ -1161,7 +1181,7 @@ __device__ __forceinline__ void tile_h_main_t(const Geo<T>& g, const StageIO<T>&
     L.s_vc[sr * RJ + scc] = (G[2] * us + G[3] * vs) * sn;
     if constexpr (RES) U.s_u[sr * RJ + scc] = us;
   }
-  if (!FULL && P > 0) edge_lines<T, S::EW>(io, b, cnt, P, L.s_np, L.s_nh, L.s_ndz);
+  if (edge_lines_staged<T>() && !FULL && P > 0) edge_lines<T, S::EW>(io, b, cnt, P, L.s_np, L.s_nh, L.s_ndz);
   __syncthreads();
 
   // faces; their fluxes (times c_dy / d_dx) alias the metric block, no longer read.  The face
