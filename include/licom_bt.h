@@ -54,6 +54,10 @@ extern "C" {
 #define BT_OPT_KERNEL_TIMING 3  /* 1 = bracket the round kernel (persistent / resident mode) or each phase
                                    kernel (stream mode) with CUDA events on its stream; setting it resets
                                    the record */
+#define BT_OPT_FULL_TILES 4  /* stream / graph mode, which phase kernels run: -1 (default) by size, the
+                                kernels with a path specialised for full interior tiles when a launch
+                                takes more than one wave of CTAs and the smaller edge-path-only kernels
+                                otherwise; 1 = always the former, 0 = always the latter (same results) */
 
 /* Kernel kinds of bt_plan_kernel_time */
 #define BT_KERNEL_ROUND 0     /* the persistent or resident round kernel */

@@ -207,10 +207,10 @@ template <typename T>
 cudaError_t run_stage(const bt_plan* p, const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
   cudaEvent_t stop;
   cudaError_t e = p->time_begin(BT_KERNEL_PHASE_H, s, &stop);
-  if (e == cudaSuccess) e = launch_phase_h<T>(g, io, p->tile, s);
+  if (e == cudaSuccess) e = launch_phase_h<T>(g, io, p->tile, s, p->full_tiles);
   if (e == cudaSuccess && stop) e = cudaEventRecord(stop, s);
   if (e == cudaSuccess) e = p->time_begin(BT_KERNEL_PHASE_UV, s, &stop);
-  if (e == cudaSuccess) e = launch_phase_uv<T>(g, io, p->tile, s);
+  if (e == cudaSuccess) e = launch_phase_uv<T>(g, io, p->tile, s, p->full_tiles);
   if (e == cudaSuccess && stop) e = cudaEventRecord(stop, s);
   return e;
 }
@@ -815,6 +815,15 @@ int bt_plan_set_option(bt_plan* p, int key, long long value) {
     case BT_OPT_KERNEL_TIMING:
       p->timing = value ? 1 : 0;
       p->tev_used = 0;
+      return BT_OK;
+    case BT_OPT_FULL_TILES:
+      if (value < -1 || value > 1) return fail(BT_EINVAL, "bt_plan_set_option: full_tiles must be -1, 0 or 1");
+      p->full_tiles = (int)value;
+      if (p->gexec) {  // the captured round holds the previous kernels
+        cudaGraphExecDestroy(p->gexec);
+        p->gexec = nullptr;
+        p->gkey.clear();
+      }
       return BT_OK;
     default:
       return fail(BT_EINVAL, "bt_plan_set_option: unknown option");

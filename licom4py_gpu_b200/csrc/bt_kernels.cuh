@@ -23,20 +23,22 @@ namespace bt {
 constexpr int kThreads = kTileThreads;
 
 
-template <typename T, int TI, int TJ>
+// FP: the full-interior-tile path compiled in (multi-wave launches), else
+// every tile runs the edge path (one-wave launches: half the code to fetch).
+template <typename T, int TI, int TJ, bool FP>
 __global__ void __launch_bounds__(kThreads, PhaseBlocks<T>::value) k_phase_h(Geo<T> g, StageIO<T> io, Tiling t) {
   extern __shared__ __align__(16) unsigned char smraw[];
   release_dependents();
   const TileBox b = tile_box(t, g.n, blockIdx.x);
-  tile_h<T, TI, TJ>(g, io, b, reinterpret_cast<T*>(smraw));
+  tile_h<T, TI, TJ, FP>(g, io, b, reinterpret_cast<T*>(smraw));
 }
 
-template <typename T, int TI, int TJ>
+template <typename T, int TI, int TJ, bool FP>
 __global__ void __launch_bounds__(kThreads, PhaseBlocksUV<T>::value) k_phase_uv(Geo<T> g, StageIO<T> io, Tiling t) {
   extern __shared__ __align__(16) unsigned char smraw[];
   release_dependents();
   const TileBox b = tile_box(t, g.n, blockIdx.x);
-  tile_uv<T, TI, TJ>(g, io, b, reinterpret_cast<T*>(smraw));
+  tile_uv<T, TI, TJ, FP>(g, io, b, reinterpret_cast<T*>(smraw));
 }
 
 // One whole round of one member in a single cooperative launch: every CTA
@@ -222,16 +224,46 @@ size_t round_smem() {
 
 // Opt in to more than 48 KB of dynamic shared memory (done at plan creation,
 // never during stream capture).
+// CTAs of one phase kernel (edge-only build) that fit on each device at once,
+// recorded by prime_tile at plan creation (0 = not recorded yet).
+constexpr int kMaxDevices = 64;
+template <typename T, int TI, int TJ, bool UV>
+int* wave_slots() {
+  static int slots[kMaxDevices] = {};
+  return slots;
+}
+
+template <typename T, int TI, int TJ, bool UV>
+cudaError_t record_wave_slots() {
+  int dev, sms, per_sm;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaSuccess;  // the launch then keeps the full-tile path
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  auto kern = UV ? k_phase_uv<T, TI, TJ, false> : k_phase_h<T, TI, TJ, false>;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, tile_smem<T, TI, TJ, UV>())) !=
+      cudaSuccess)
+    return e;
+  wave_slots<T, TI, TJ, UV>()[dev] = sms * per_sm;
+  return cudaSuccess;
+}
+
 template <typename T, int TI, int TJ>
 cudaError_t prime_tile() {
-  cudaError_t e = cudaFuncSetAttribute(k_phase_h<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)tile_smem<T, TI, TJ, false>());
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  for (auto k : {k_phase_h<T, TI, TJ, true>, k_phase_h<T, TI, TJ, false>})
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tile_smem<T, TI, TJ, false>())) != cudaSuccess)
+      return e;
+  for (auto k : {k_phase_uv<T, TI, TJ, true>, k_phase_uv<T, TI, TJ, false>})
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)tile_smem<T, TI, TJ, true>())) != cudaSuccess)
+      return e;
   e = cudaFuncSetAttribute(k_round<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)round_smem<T, TI, TJ>());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_phase_uv<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)tile_smem<T, TI, TJ, true>());
+  if ((e = record_wave_slots<T, TI, TJ, false>()) != cudaSuccess) return e;
+  return record_wave_slots<T, TI, TJ, true>();
 }
 
 // Co-resident grid for the persistent kernel (at most one CTA per tile).
@@ -255,10 +287,18 @@ cudaError_t launch_round_tile(RoundArgs<T> a, int max_ctas, cudaStream_t s, int*
 }
 
 template <typename T, int TI, int TJ, bool UV>
-cudaError_t launch_tile(const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
+cudaError_t launch_tile(const Geo<T>& g, const StageIO<T>& io, cudaStream_t s, int full_tiles) {
   const size_t smem = tile_smem<T, TI, TJ, UV>();
-  auto kern = UV ? k_phase_uv<T, TI, TJ> : k_phase_h<T, TI, TJ>;
   const Tiling t = make_tiling({TI, TJ}, g.n);
+  bool fp = full_tiles != 0;
+  if (full_tiles < 0) {  // by size: edge-only kernel when the launch is one wave
+    int dev = -1;
+    const int slots = (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices)
+                          ? wave_slots<T, TI, TJ, UV>()[dev] : 0;
+    fp = !(slots > 0 && 6 * t.tiles_per_face() <= slots);
+  }
+  auto kern = UV ? (fp ? k_phase_uv<T, TI, TJ, true> : k_phase_uv<T, TI, TJ, false>)
+                 : (fp ? k_phase_h<T, TI, TJ, true> : k_phase_h<T, TI, TJ, false>);
   // programmatic dependent launch: the kernel's constant prologue overlaps the
   // previous kernel's tail; it waits (griddepcontrol.wait) before reading state
   cudaLaunchConfig_t cfg = {};
@@ -275,13 +315,13 @@ cudaError_t launch_tile(const Geo<T>& g, const StageIO<T>& io, cudaStream_t s) {
 }
 
 template <typename T, bool UV>
-cudaError_t dispatch(const Geo<T>& g, const StageIO<T>& io, TileCfg c, cudaStream_t s) {
-  if (c.ti == 7 && c.tj == 32) return launch_tile<T, 7, 32, UV>(g, io, s);
-  if (c.ti == 8 && c.tj == 32) return launch_tile<T, 8, 32, UV>(g, io, s);
-  if (c.ti == 15 && c.tj == 32) return launch_tile<T, 15, 32, UV>(g, io, s);
-  if (c.ti == 16 && c.tj == 32) return launch_tile<T, 16, 32, UV>(g, io, s);
-  if (c.ti == 8 && c.tj == 16) return launch_tile<T, 8, 16, UV>(g, io, s);
-  if (c.ti == 16 && c.tj == 16) return launch_tile<T, 16, 16, UV>(g, io, s);
+cudaError_t dispatch(const Geo<T>& g, const StageIO<T>& io, TileCfg c, cudaStream_t s, int full_tiles) {
+  if (c.ti == 7 && c.tj == 32) return launch_tile<T, 7, 32, UV>(g, io, s, full_tiles);
+  if (c.ti == 8 && c.tj == 32) return launch_tile<T, 8, 32, UV>(g, io, s, full_tiles);
+  if (c.ti == 15 && c.tj == 32) return launch_tile<T, 15, 32, UV>(g, io, s, full_tiles);
+  if (c.ti == 16 && c.tj == 32) return launch_tile<T, 16, 32, UV>(g, io, s, full_tiles);
+  if (c.ti == 8 && c.tj == 16) return launch_tile<T, 8, 16, UV>(g, io, s, full_tiles);
+  if (c.ti == 16 && c.tj == 16) return launch_tile<T, 16, 16, UV>(g, io, s, full_tiles);
   return cudaErrorInvalidValue;
 }
 
@@ -310,13 +350,13 @@ cudaError_t prime_kernels() {
 }
 
 template <typename T>
-cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s) {
-  return dispatch<T, false>(g, io, cfg, s);
+cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s, int full_tiles) {
+  return dispatch<T, false>(g, io, cfg, s, full_tiles);
 }
 
 template <typename T>
-cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s) {
-  return dispatch<T, true>(g, io, cfg, s);
+cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s, int full_tiles) {
+  return dispatch<T, true>(g, io, cfg, s, full_tiles);
 }
 
 template <typename T, int TI, int TJ>
@@ -356,8 +396,8 @@ cudaError_t launch_diag(const Geo<T>& g, const T* h, const T* u, const T* v, con
 
 #define BT_INSTANTIATE(T)                                                                           \
   template cudaError_t prime_kernels<T>();                                                          \
-  template cudaError_t launch_phase_h<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t);  \
-  template cudaError_t launch_phase_uv<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t); \
+  template cudaError_t launch_phase_h<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t, int);  \
+  template cudaError_t launch_phase_uv<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t, int); \
   template cudaError_t launch_fill_halo<T>(const Geo<T>&, T*, T*, T*, cudaStream_t);                \
   template cudaError_t launch_const_blocks<T>(const Geo<T>&, TileCfg, T*, cudaStream_t);               \
   template cudaError_t launch_round<T>(const RoundArgs<T>&, TileCfg, int, cudaStream_t, int*);      \

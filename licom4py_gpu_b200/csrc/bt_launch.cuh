@@ -30,10 +30,14 @@ Tiling make_tiling(TileCfg c, int n);
 // Set kernel attributes (dynamic shared memory opt-in) for the current device.
 template <typename T>
 cudaError_t prime_kernels();
+// Phase kernels of one stage.  full_tiles selects the kernel: 1 = the one with
+// the full-interior-tile path, 0 = edge path only, -1 = by size (the edge-only
+// kernel when the launch's CTAs all fit on the device at once).  Results are
+// the same either way.
 template <typename T>
-cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s);
+cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s, int full_tiles = -1);
 template <typename T>
-cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s);
+cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s, int full_tiles = -1);
 // Persistent cooperative launch of a whole round (phases of all substeps);
 // max_ctas > 0 caps the grid.  The grid size used is returned in *grid_out.
 template <typename T>

@@ -68,6 +68,7 @@ struct bt_plan {
   unsigned* d_flags = nullptr;  // [0] barrier counter, [1] error bits
   int max_ctas = 0;
   long long spin_limit = 1ll << 24;
+  int full_tiles = -1;  // BT_OPT_FULL_TILES
   int last_grid = 0;
   // optional kernel timing: event pairs on the launch stream around the round
   // kernel (persistent mode) or each phase kernel (stream mode), with their kind

@@ -1510,60 +1510,65 @@ __device__ __forceinline__ void tile_uv_main_t(const Geo<T>& g, const StageIO<T>
   }
 }
 
-// Tile phases dispatched on the tile's kind: full interior tiles run the
-// FULL = true instantiation.  Prologue and main part of one tile must take
-// the same branch, which they do since both test the same tile box.
-template <typename T, int TI, int TJ>
+// Tile phases dispatched on the tile's kind: with FP (the full-tile path
+// compiled in), full interior tiles run the FULL = true instantiation and the
+// others the edge instantiation; without it every tile runs the edge
+// instantiation, which handles full tiles too.  The kernel without the full
+// path is about half the code: at one-wave sizes (every CTA runs the code
+// once, and instruction fetch is the largest stall) it is the faster one.
+// Prologue and main part of one tile take the same branch, since both test
+// the same tile box.
+template <typename T, int TI, int TJ, bool FP = true>
 __device__ __forceinline__ void tile_h_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
                                            Gather<T, TI, TJ, false>& gat, EdgeCnt& cnt, int& P) {
-  if (tile_full(b, g.m, TI, TJ))
+  if (FP && tile_full(b, g.m, TI, TJ))
     tile_h_pro_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
     tile_h_pro_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
 }
-template <typename T, int TI, int TJ>
+template <typename T, int TI, int TJ, bool FP = true>
 __device__ __forceinline__ void tile_h_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
                                             Gather<T, TI, TJ, false>& gat, const EdgeCnt& cnt, int P) {
-  if (tile_full(b, g.m, TI, TJ))
+  if (FP && tile_full(b, g.m, TI, TJ))
     tile_h_main_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
     tile_h_main_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
 }
-template <typename T, int TI, int TJ>
+template <typename T, int TI, int TJ, bool FP = true>
 __device__ __forceinline__ void tile_uv_pro(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
                                             Gather<T, TI, TJ, true>& gat, EdgeCnt& cnt, int& P) {
-  if (tile_full(b, g.m, TI, TJ))
+  if (FP && tile_full(b, g.m, TI, TJ))
     tile_uv_pro_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
     tile_uv_pro_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
 }
-template <typename T, int TI, int TJ>
+template <typename T, int TI, int TJ, bool FP = true>
 __device__ __forceinline__ void tile_uv_main(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm,
                                              Gather<T, TI, TJ, true>& gat, const EdgeCnt& cnt, int P) {
-  if (tile_full(b, g.m, TI, TJ))
+  if (FP && tile_full(b, g.m, TI, TJ))
     tile_uv_main_t<T, TI, TJ, true>(g, io, b, sm, gat, cnt, P);
   else
     tile_uv_main_t<T, TI, TJ, false>(g, io, b, sm, gat, cnt, P);
 }
 
 // One tile phase with the prologue issued first (the stream/graph kernels).
-template <typename T, int TI, int TJ>
+template <typename T, int TI, int TJ, bool FP = true>
 __device__ __forceinline__ void tile_h(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
   Gather<T, TI, TJ, false> gat;
   EdgeCnt cnt;
   int P;
-  tile_h_pro<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+  tile_h_pro<T, TI, TJ, FP>(g, io, b, sm, gat, cnt, P);
   wait_prior_grid();
-  tile_h_main<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+  tile_h_main<T, TI, TJ, FP>(g, io, b, sm, gat, cnt, P);
 }
-template <typename T, int TI, int TJ>
+template <typename T, int TI, int TJ, bool FP = true>
 __device__ __forceinline__ void tile_uv(const Geo<T>& g, const StageIO<T>& io, const TileBox& b, T* sm) {
   Gather<T, TI, TJ, true> gat;
   EdgeCnt cnt;
   int P;
-  tile_uv_pro<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+  tile_uv_pro<T, TI, TJ, FP>(g, io, b, sm, gat, cnt, P);
   wait_prior_grid();
-  tile_uv_main<T, TI, TJ>(g, io, b, sm, gat, cnt, P);
+  tile_uv_main<T, TI, TJ, FP>(g, io, b, sm, gat, cnt, P);
 }
 
 

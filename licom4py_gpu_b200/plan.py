@@ -122,6 +122,13 @@ class BtPlan:
         (stream mode) with CUDA events on its stream; resets the record."""
         self.set_option(N.BT_OPT_KERNEL_TIMING, 1 if on else 0)
 
+    def set_full_tiles(self, which) -> None:
+        """Stream / graph mode phase kernels: None (default) by size -- the kernels with a
+        path specialised for full interior tiles when a launch takes more than one wave of
+        CTAs, the smaller edge-path-only kernels otherwise; True / False forces one of them.
+        The results are the same."""
+        self.set_option(N.BT_OPT_FULL_TILES, -1 if which is None else (1 if which else 0))
+
     KERNELS = {"round": N.BT_KERNEL_ROUND, "phase_h": N.BT_KERNEL_PHASE_H, "phase_uv": N.BT_KERNEL_PHASE_UV}
 
     def kernel_time(self, kind: str = "round") -> Tuple[float, int]:

@@ -299,8 +299,10 @@ def test_misaligned_constant_views_give_the_same_round(grids):
 
 # Tiles of 32 columns have full interior tiles (the whole stencil region inside
 # the face, compiled without the edge logic) only from C96 on; these cases run
-# every full-tile instantiation next to edge tiles.
-@pytest.mark.parametrize("tile", [(7, 32), (8, 32), (15, 32), (16, 32), (16, 16)])
+# every full-tile instantiation next to edge tiles.  A C96 launch is one wave,
+# where the plan would pick the edge-path-only kernels, so the full-tile kernels
+# are forced here and compared with the edge-path-only kernels of the 8 x 16 tile.
+@pytest.mark.parametrize("tile", [(7, 32), (8, 32), (15, 32), (16, 32), (8, 16), (16, 16)])
 def test_full_tile_shapes_bitwise_identical_c96(tile, grids):
     g = grids(96)
     consts = make_consts(g, 5000.0)
@@ -308,6 +310,8 @@ def test_full_tile_shapes_bitwise_identical_c96(tile, grids):
     ins = [dev(s["h0"]), dev(s["h0"]), dev(s["ub"]), dev(s["vb"]), dev(s["ub"]), dev(s["vb"])]
     dtb = cfl_dtb(g, 5000.0)
     ref_plan, plan = BtPlan(consts, tile=(8, 16)), BtPlan(consts, tile=tile)
+    ref_plan.set_full_tiles(False)
+    plan.set_full_tiles(True)
     for rk in (2, 3):
         ref = ref_plan.round(*ins, nbb=3, dtb=dtb, rk=rk)
         got = plan.round(*ins, nbb=3, dtb=dtb, rk=rk)
@@ -329,11 +333,34 @@ def test_float32_full_tiles_c96(tile, grids):
     p64 = BtPlan(consts, tile=(8, 16))
     want = p64.round(*[dev(s[k]) for k in keys], nbb=100, dtb=dtb, diag=False)
     p32 = BtPlan(consts, dtype=torch.float32, tile=tile)
-    got = p32.round(*[dev(s[k], torch.float32) for k in keys], nbb=100, dtb=dtb, diag=False)
-    for key in ("h0", "ub", "vb"):
-        a = got[key][:, 3:-3, 3:-3].double()
-        b = want[key][:, 3:-3, 3:-3]
-        l2 = ((a - b).norm() / b.norm()).item()
-        assert l2 <= 1e-5, f"{tile} {key}: relative L2 error {l2:.2e}"
+    for full in (True, False):  # the full-tile kernels, then the edge-path-only kernels
+        p32.set_full_tiles(full)
+        got = p32.round(*[dev(s[k], torch.float32) for k in keys], nbb=100, dtb=dtb, diag=False)
+        for key in ("h0", "ub", "vb"):
+            a = got[key][:, 3:-3, 3:-3].double()
+            b = want[key][:, 3:-3, 3:-3]
+            l2 = ((a - b).norm() / b.norm()).item()
+            assert l2 <= 1e-5, f"{tile} full={full} {key}: relative L2 error {l2:.2e}"
     p64.close()
     p32.close()
+
+
+@pytest.mark.parametrize("n,tile", [(48, (8, 16)), (96, (8, 16)), (192, (8, 32)), (384, (16, 32))])
+def test_full_tile_choice_gives_the_same_round(n, tile, grids):
+    """The kernel chosen by size, the full-tile kernels and the edge-path-only kernels give
+    bit-identical float64 rounds (graph mode, RK2 and RK3)."""
+    g = grids(n)
+    consts = make_consts(g, 5000.0)
+    s = harmonic_state(g, 21)
+    ins = [dev(s["h0"]), dev(s["h0"]), dev(s["ub"]), dev(s["vb"]), dev(s["ub"]), dev(s["vb"])]
+    dtb = cfl_dtb(g, 5000.0)
+    plan = BtPlan(consts, tile=tile, mode="graph")
+    for rk in (2, 3):
+        outs = []
+        for full in (None, True, False):
+            plan.set_full_tiles(full)
+            outs.append(plan.round(*ins, nbb=2, dtb=dtb, rk=rk, diag=False))
+        for got in outs[1:]:
+            for k in outs[0]:
+                assert torch.equal(outs[0][k], got[k]), (n, tile, rk, k)
+    plan.close()
