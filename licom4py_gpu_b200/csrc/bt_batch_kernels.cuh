@@ -130,8 +130,10 @@ __device__ __forceinline__ int active_members(const BatchArgs<T>& a, int act, in
 constexpr int kBatchPhaseBlocks = 3;
 
 // Tile phase of every active member (one launch per phase): blockIdx.x is the
-// tile in the member-major tile list.
-template <typename T, int TI, int TJ, bool UV>
+// tile in the member-major tile list.  FP: the full-interior-tile path
+// compiled in (launches of more than one wave), else the smaller edge-path-only
+// code (launches whose CTAs all fit at once).
+template <typename T, int TI, int TJ, bool UV, bool FP>
 __global__ void __launch_bounds__(kTileThreads, kBatchPhaseBlocks) k_batch_phase(BatchArgs<T> a, int step, int st, int act) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ TileCtx<T> ctx;
@@ -150,9 +152,9 @@ __global__ void __launch_bounds__(kTileThreads, kBatchPhaseBlocks) k_batch_phase
   const TileBox b = tile_box_at(make_tiling_dev(TI, TJ, g.n), g.n, tile - __ldg(a.off.tile + k));
   T* sm = reinterpret_cast<T*>(smraw);
   if (!UV)
-    tile_h<T, TI, TJ>(g, ctx.io, b, sm);
+    tile_h<T, TI, TJ, FP>(g, ctx.io, b, sm);
   else
-    tile_uv<T, TI, TJ>(g, ctx.io, b, sm);
+    tile_uv<T, TI, TJ, FP>(g, ctx.io, b, sm);
 }
 
 // End of a round: halo fill of every member's output and, for members with
@@ -271,14 +273,38 @@ size_t batch_round_smem() {
   return std::max(batch_tile_smem<T, TI, TJ, false>(), batch_tile_smem<T, TI, TJ, true>());
 }
 
+// CTAs of one batched phase kernel (edge-only build) that fit on each device
+// at once, recorded by prime_batch_tile (0 = not recorded).
+constexpr int kMaxBatchDevices = 64;
+template <typename T, int TI, int TJ, bool UV>
+int* batch_wave_slots() {
+  static int slots[kMaxBatchDevices] = {};
+  return slots;
+}
+
+template <typename T, int TI, int TJ, bool UV>
+cudaError_t prime_batch_phase() {
+  cudaError_t e;
+  for (auto k : {k_batch_phase<T, TI, TJ, UV, true>, k_batch_phase<T, TI, TJ, UV, false>})
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)batch_tile_smem<T, TI, TJ, UV>())) != cudaSuccess)
+      return e;
+  int dev, sms, per_sm;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxBatchDevices) return cudaSuccess;  // launches then keep the full-tile path
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_phase<T, TI, TJ, UV, false>, kTileThreads,
+                                                         batch_tile_smem<T, TI, TJ, UV>())) != cudaSuccess)
+    return e;
+  batch_wave_slots<T, TI, TJ, UV>()[dev] = sms * per_sm;
+  return cudaSuccess;
+}
+
 template <typename T, int TI, int TJ>
 cudaError_t prime_batch_tile() {
-  cudaError_t e = cudaFuncSetAttribute(k_batch_phase<T, TI, TJ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)batch_tile_smem<T, TI, TJ, false>());
+  cudaError_t e = prime_batch_phase<T, TI, TJ, false>();
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_batch_phase<T, TI, TJ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)batch_tile_smem<T, TI, TJ, true>());
-  if (e != cudaSuccess) return e;
+  if ((e = prime_batch_phase<T, TI, TJ, true>()) != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_batch_round<T, TI, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)batch_round_smem<T, TI, TJ>());
 }
@@ -317,7 +343,12 @@ cudaError_t launch_batch_phase_tile(const BatchArgs<T>& a, int step, int st, int
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_batch_phase<T, TI, TJ, UV>, a, step, st, act);
+  int dev = -1;
+  const int slots = (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxBatchDevices)
+                        ? batch_wave_slots<T, TI, TJ, UV>()[dev] : 0;
+  const bool one_wave = slots > 0 && ntiles <= slots;
+  return one_wave ? cudaLaunchKernelEx(&cfg, k_batch_phase<T, TI, TJ, UV, false>, a, step, st, act)
+                  : cudaLaunchKernelEx(&cfg, k_batch_phase<T, TI, TJ, UV, true>, a, step, st, act);
 }
 
 template <typename T, bool UV>
