@@ -675,6 +675,7 @@ def run_ours(args, world, rank, local):
         p.round(h, h, u, v, u, v, nbb=nbb_, dtb=dtb_, out=o)
         torch.cuda.synchronize()
         res = {k: p.kernel_time(k) for k in ("phase_h", "phase_uv")}
+        fp = dict(zip(("phase_h", "phase_uv"), p.full_tile_kernels))  # which build of each kernel ran
         p.close()
         tot = sum(ms for ms, _ in res.values())
         dom = max(res, key=lambda k: res[k][0])
@@ -690,7 +691,7 @@ def run_ours(args, world, rank, local):
             except (OSError, ValueError):
                 traffic = None
         return {"bound": "hbm", "kernel": f"{KERNEL_NAMES[dom]}<{'double' if esz == 8 else 'float'},"
-                                          f"{tile_[0]},{tile_[1]}>",
+                                          f"{tile_[0]},{tile_[1]},{'true' if fp[dom] else 'false'}>",
                 "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "launch_us": 1e3 * ms / nl,
                 "alg_bytes_per_launch": alg, "launches_timed": nl,

@@ -67,6 +67,8 @@ extern "C" {
 /* Plan information (bt_plan_get_info) */
 #define BT_INFO_LAST_GRID 1      /* CTAs of the last persistent launch */
 #define BT_INFO_SCRATCH_BYTES 2  /* device scratch owned by the plan */
+#define BT_INFO_FULL_TILES 3     /* stream / graph mode phase kernels at the plan's tile and size: bit 0 set =
+                                    phase H runs the kernel with the full-tile path, bit 1 = phase UV */
 
 typedef struct bt_plan bt_plan;
 

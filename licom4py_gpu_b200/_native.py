@@ -16,7 +16,7 @@ BT_OK, BT_EINVAL, BT_ENOMEM, BT_ECUDA, BT_EDEVICE, BT_ENOTSUP = 0, -1, -2, -3, -
 BT_F64, BT_F32 = 0, 1
 BT_MODE_STREAM, BT_MODE_GRAPH, BT_MODE_PERSISTENT, BT_MODE_RESIDENT = 0, 1, 2, 3
 BT_OPT_MAX_CTAS, BT_OPT_SPIN_LIMIT, BT_OPT_KERNEL_TIMING, BT_OPT_FULL_TILES = 1, 2, 3, 4
-BT_INFO_LAST_GRID, BT_INFO_SCRATCH_BYTES = 1, 2
+BT_INFO_LAST_GRID, BT_INFO_SCRATCH_BYTES, BT_INFO_FULL_TILES = 1, 2, 3
 BT_KERNEL_ROUND, BT_KERNEL_PHASE_H, BT_KERNEL_PHASE_UV = 0, 1, 2
 
 _vp = ctypes.c_void_p

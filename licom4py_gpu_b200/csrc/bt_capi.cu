@@ -852,6 +852,15 @@ long long bt_plan_get_info(bt_plan* p, int key) {
   switch (key) {
     case BT_INFO_LAST_GRID: return p->last_grid;
     case BT_INFO_SCRATCH_BYTES: return (long long)p->scratch_bytes();
+    case BT_INFO_FULL_TILES: {  // evaluated on the plan's device, as its launches are
+      int cur = -1;
+      cudaGetDevice(&cur);
+      if (cur != p->device) cudaSetDevice(p->device);
+      const int r = p->dtype == BT_F64 ? phase_full_paths<double>(p->tile, p->n, p->full_tiles)
+                                       : phase_full_paths<float>(p->tile, p->n, p->full_tiles);
+      if (cur >= 0 && cur != p->device) cudaSetDevice(cur);
+      return r;
+    }
     default: return -1;
   }
 }

@@ -286,17 +286,23 @@ cudaError_t launch_round_tile(RoundArgs<T> a, int max_ctas, cudaStream_t s, int*
   return cudaLaunchCooperativeKernel((const void*)k_round<T, TI, TJ>, dim3(grid), dim3(kThreads), args, smem, s);
 }
 
+// Whether a phase launch at n cells per face edge runs the full-tile kernel:
+// forced by full_tiles >= 0, else by size (the edge-only kernel when the
+// launch's CTAs all fit on the current device at once).
+template <typename T, int TI, int TJ, bool UV>
+bool full_path(int n, int full_tiles) {
+  if (full_tiles >= 0) return full_tiles != 0;
+  int dev = -1;
+  const int slots =
+      (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) ? wave_slots<T, TI, TJ, UV>()[dev] : 0;
+  return !(slots > 0 && 6 * make_tiling({TI, TJ}, n).tiles_per_face() <= slots);
+}
+
 template <typename T, int TI, int TJ, bool UV>
 cudaError_t launch_tile(const Geo<T>& g, const StageIO<T>& io, cudaStream_t s, int full_tiles) {
   const size_t smem = tile_smem<T, TI, TJ, UV>();
   const Tiling t = make_tiling({TI, TJ}, g.n);
-  bool fp = full_tiles != 0;
-  if (full_tiles < 0) {  // by size: edge-only kernel when the launch is one wave
-    int dev = -1;
-    const int slots = (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices)
-                          ? wave_slots<T, TI, TJ, UV>()[dev] : 0;
-    fp = !(slots > 0 && 6 * t.tiles_per_face() <= slots);
-  }
+  const bool fp = full_path<T, TI, TJ, UV>(g.n, full_tiles);
   auto kern = UV ? (fp ? k_phase_uv<T, TI, TJ, true> : k_phase_uv<T, TI, TJ, false>)
                  : (fp ? k_phase_h<T, TI, TJ, true> : k_phase_h<T, TI, TJ, false>);
   // programmatic dependent launch: the kernel's constant prologue overlaps the
@@ -350,6 +356,21 @@ cudaError_t prime_kernels() {
 }
 
 template <typename T>
+int phase_full_paths(TileCfg c, int n, int full_tiles) {
+#define BT_FP_BITS(TI, TJ) \
+  if (c.ti == TI && c.tj == TJ) \
+    return (full_path<T, TI, TJ, false>(n, full_tiles) ? 1 : 0) | (full_path<T, TI, TJ, true>(n, full_tiles) ? 2 : 0);
+  BT_FP_BITS(7, 32)
+  BT_FP_BITS(8, 32)
+  BT_FP_BITS(15, 32)
+  BT_FP_BITS(16, 32)
+  BT_FP_BITS(8, 16)
+  BT_FP_BITS(16, 16)
+#undef BT_FP_BITS
+  return -1;
+}
+
+template <typename T>
 cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s, int full_tiles) {
   return dispatch<T, false>(g, io, cfg, s, full_tiles);
 }
@@ -396,6 +417,7 @@ cudaError_t launch_diag(const Geo<T>& g, const T* h, const T* u, const T* v, con
 
 #define BT_INSTANTIATE(T)                                                                           \
   template cudaError_t prime_kernels<T>();                                                          \
+  template int phase_full_paths<T>(TileCfg, int, int);                                              \
   template cudaError_t launch_phase_h<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t, int);  \
   template cudaError_t launch_phase_uv<T>(const Geo<T>&, const StageIO<T>&, TileCfg, cudaStream_t, int); \
   template cudaError_t launch_fill_halo<T>(const Geo<T>&, T*, T*, T*, cudaStream_t);                \

@@ -36,6 +36,10 @@ cudaError_t prime_kernels();
 // the same either way.
 template <typename T>
 cudaError_t launch_phase_h(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s, int full_tiles = -1);
+// Which kernels those launches take at n: bit 0 set = phase H runs the full-tile
+// kernel, bit 1 = phase UV (-1: unsupported tile shape).
+template <typename T>
+int phase_full_paths(TileCfg cfg, int n, int full_tiles);
 template <typename T>
 cudaError_t launch_phase_uv(const Geo<T>& g, const StageIO<T>& io, TileCfg cfg, cudaStream_t s, int full_tiles = -1);
 // Persistent cooperative launch of a whole round (phases of all substeps);

@@ -146,6 +146,13 @@ class BtPlan:
     def scratch_bytes(self) -> int:
         return int(N.lib().bt_plan_get_info(self._h, N.BT_INFO_SCRATCH_BYTES))
 
+    @property
+    def full_tile_kernels(self) -> Tuple[bool, bool]:
+        """(phase H, phase UV): whether the stream / graph mode launches at this plan's tile and
+        size run the kernels with the full-tile path (else the edge-path-only kernels)."""
+        bits = int(N.lib().bt_plan_get_info(self._h, N.BT_INFO_FULL_TILES))
+        return bool(bits & 1), bool(bits & 2)
+
     # -- validation --------------------------------------------------------------
     def _check_field(self, name: str, t: torch.Tensor) -> None:
         if not isinstance(t, torch.Tensor):

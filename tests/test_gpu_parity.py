@@ -355,6 +355,10 @@ def test_full_tile_choice_gives_the_same_round(n, tile, grids):
     ins = [dev(s["h0"]), dev(s["h0"]), dev(s["ub"]), dev(s["vb"]), dev(s["ub"]), dev(s["vb"])]
     dtb = cfl_dtb(g, 5000.0)
     plan = BtPlan(consts, tile=tile, mode="graph")
+    plan.set_full_tiles(True)
+    assert plan.full_tile_kernels == (True, True)
+    plan.set_full_tiles(False)
+    assert plan.full_tile_kernels == (False, False)
     for rk in (2, 3):
         outs = []
         for full in (None, True, False):
