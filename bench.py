@@ -455,7 +455,14 @@ def form_ensemble(dev, depth):
     from licom4py_gpu_b200.batch import BtBatch
     from licom4py_gpu_b200.duogrid import make_consts
     from licom4py_gpu_b200.ensemble import Ensemble, Geometry, PlainRunner, uneven_mix
+    import multiprocessing as mp
     specs = uneven_mix()
+    # part of the CPU-baseline leg: the float64 oracle runs the 4 shortest C48 members (same seeded
+    # initial states and CFL step) in a spawned host process while the GPU runs the ensemble
+    pick = sorted(range(len(specs)), key=lambda k: (specs[k].n, specs[k].nsub))[:4]
+    pool = mp.get_context("spawn").Pool(1)
+    oracle_job = pool.apply_async(_oracle_requests, (depth, [(specs[k].n, specs[k].nsub, specs[k].seed,
+                                                              specs[k].amplitude) for k in pick]))
     geo = Geometry(depth, device=dev)
     ens = Ensemble(specs, torch.float32, geometry=geo)
     cfg = autotune.choose_batch_config(ens)
@@ -491,6 +498,13 @@ def form_ensemble(dev, depth):
     torch.cuda.synchronize()
     l2 = max(_rel(a.state[0], c.state[0])[0] for a, c in zip(mem32, mem64))
     li = max(_rel(a.state[0], c.state[0])[1] for a, c in zip(mem32, mem64))
+    try:
+        want = oracle_job.get(timeout=900)
+        vs_oracle = max(_rel(mem32[k].state[0], torch.from_numpy(w).to(dev))[0] for k, w in zip(pick, want))
+    except Exception as e:  # a report, not a failure of the bench
+        vs_oracle = f"oracle run did not finish: {type(e).__name__}"
+    finally:
+        pool.terminate()
     b.close()
     b64.close()
     geo.close()
@@ -502,7 +516,8 @@ def form_ensemble(dev, depth):
                                                            if k in cfg}},
             "plain_one_per_launch": {"value": vp, "unit": UNIT, "ms": ms_p,
                                      "configs": {str(k): [v["mode"], v["tile"]] for k, v in singles.items()}},
-            "speedup": vb / vp, "h_rel_l2_max_vs_f64": l2, "h_rel_linf_max_vs_f64": li}
+            "speedup": vb / vp, "h_rel_l2_max_vs_f64": l2, "h_rel_linf_max_vs_f64": li,
+            "h_rel_l2_vs_oracle_shortest4_c48": vs_oracle}
 
 
 def form_serving(dev, depth, count):
