@@ -26,7 +26,7 @@ constexpr int kThreads = kTileThreads;
 // FP: the full-interior-tile path compiled in (multi-wave launches), else
 // every tile runs the edge path (one-wave launches: half the code to fetch).
 template <typename T, int TI, int TJ, bool FP>
-__global__ void __launch_bounds__(kThreads, PhaseBlocks<T>::value) k_phase_h(Geo<T> g, StageIO<T> io, Tiling t) {
+__global__ void __launch_bounds__(kThreads, PhaseBlocks<T, FP>::value) k_phase_h(Geo<T> g, StageIO<T> io, Tiling t) {
   extern __shared__ __align__(16) unsigned char smraw[];
   release_dependents();
   const TileBox b = tile_box(t, g.n, blockIdx.x);

@@ -206,11 +206,14 @@ __device__ __forceinline__ int yface_side(int j, int m) {
 // cp.async in a prologue that does not depend on the state.
 constexpr int kTileThreads = 256;
 
-// Resident CTAs per SM the tile-phase kernels are compiled for (register cap
-// 65536 / (256 * blocks)): float64 tiles need more registers per thread.
-template <typename T>
+// Resident CTAs per SM the phase H kernels are compiled for (register cap
+// 65536 / (256 * blocks)): float64 tiles need more registers per thread.  The
+// float32 build with the full-tile path runs 4 (multi-wave launches: C384 7 %
+// faster than at 3); the edge-path-only build, which runs the one-wave launches,
+// 3 (C96 8 x 16 13.15 -> 11.93 us per substep, C48 12.43 -> 11.51).
+template <typename T, bool FP = true>
 struct PhaseBlocks {
-  static constexpr int value = sizeof(T) == 8 ? 3 : 4;
+  static constexpr int value = sizeof(T) == 8 ? 3 : (FP ? 4 : 3);
 };
 // Phase UV runs 3 CTAs per SM in both precisions: at 4 its shared-memory
 // traffic throttles (MIO) and the best tile shape per size measured faster at 3.
