@@ -15,6 +15,7 @@ from helpers import STAGE_OUT, STATE_KEYS, golden_inputs, rel_err
 from licom4py_gpu_b200 import barotr, barotr_pure
 from licom4py_gpu_b200.duogrid import make_consts
 from licom4py_gpu_b200.fields import cfl_dtb, harmonic_state
+from licom4py_gpu_b200 import _native as N
 from licom4py_gpu_b200.plan import DIAG_NAMES, BtPlan
 from oracle import barotr_np as O
 
@@ -359,6 +360,9 @@ def test_full_tile_choice_gives_the_same_round(n, tile, grids):
     assert plan.full_tile_kernels == (True, True)
     plan.set_full_tiles(False)
     assert plan.full_tile_kernels == (False, False)
+    for bad in (-2, 2):
+        with pytest.raises(ValueError):
+            plan.set_option(N.BT_OPT_FULL_TILES, bad)
     for rk in (2, 3):
         outs = []
         for full in (None, True, False):
