@@ -19,7 +19,7 @@ outputs are committed as ``tests/golden/*.npz``; the tests never import the
 reference.  Each fixture records the SHA-256 of the float64 constants it was
 made with so the tests can check that the generator still reproduces them.
 
-Usage:  python tests/golden/make_golden.py --ref PATH_TO_REFERENCE
+Usage:  python tests/golden/make_golden.py --ref PATH_TO_REFERENCE [--only NAME.npz ...]
         (or set LICOM_REFERENCE_ROOT to the reference checkout)
 """
 
@@ -197,19 +197,30 @@ def main():
     p.add_argument("--ref", default=os.environ.get("LICOM_REFERENCE_ROOT"),
                    help="root of the reference checkout (default: $LICOM_REFERENCE_ROOT)")
     p.add_argument("--out", default=HERE)
+    p.add_argument("--only", nargs="*", default=None,
+                   help="fixture file names to (re)generate; default: all of them")
     a = p.parse_args()
     if not a.ref:
         p.error("give --ref PATH_TO_REFERENCE or set LICOM_REFERENCE_ROOT")
-    gen_halo(a.ref, a.out)
-    gen_stage(a.ref, a.out)
-    gen_core(a.ref, a.out, "rk2_c8.npz", n=8, nbb=4, seed=1)
-    gen_core(a.ref, a.out, "rk2_c12_base.npz", n=12, nbb=3, seed=2, base_seed=3)
-    gen_core(a.ref, a.out, "rk3_c8.npz", n=8, nbb=3, seed=4, rk=3)
-    gen_core(a.ref, a.out, "rk2_c8_nbb0.npz", n=8, nbb=0, seed=5)
-    gen_core(a.ref, a.out, "rk2_c24.npz", n=24, nbb=10, seed=6, keep_inputs=False,
-             outputs=STATE_KEYS[:16])
-    gen_core(a.ref, a.out, "rk2_c48_100.npz", n=48, nbb=100, seed=7, keep_inputs=False,
-             outputs=("h0", "ub", "vb"))
+    jobs = {
+        "halo.npz": lambda: gen_halo(a.ref, a.out),
+        "stage_c8.npz": lambda: gen_stage(a.ref, a.out),
+        "rk2_c8.npz": lambda: gen_core(a.ref, a.out, "rk2_c8.npz", n=8, nbb=4, seed=1),
+        "rk2_c12_base.npz": lambda: gen_core(a.ref, a.out, "rk2_c12_base.npz", n=12, nbb=3, seed=2, base_seed=3),
+        "rk3_c8.npz": lambda: gen_core(a.ref, a.out, "rk3_c8.npz", n=8, nbb=3, seed=4, rk=3),
+        "rk2_c8_nbb0.npz": lambda: gen_core(a.ref, a.out, "rk2_c8_nbb0.npz", n=8, nbb=0, seed=5),
+        "rk2_c24.npz": lambda: gen_core(a.ref, a.out, "rk2_c24.npz", n=24, nbb=10, seed=6, keep_inputs=False,
+                                        outputs=STATE_KEYS[:16]),
+        "rk2_c48_100.npz": lambda: gen_core(a.ref, a.out, "rk2_c48_100.npz", n=48, nbb=100, seed=7,
+                                            keep_inputs=False, outputs=("h0", "ub", "vb")),
+        # RK3 where tiles of the 8 x 16 and 16 x 16 shapes are full interior tiles
+        "rk3_c48_30.npz": lambda: gen_core(a.ref, a.out, "rk3_c48_30.npz", n=48, nbb=30, seed=8, rk=3,
+                                           keep_inputs=False, outputs=("h0", "ub", "vb")),
+    }
+    for name in (a.only if a.only else jobs):
+        if name not in jobs:
+            p.error(f"unknown fixture {name}; known: {', '.join(jobs)}")
+        jobs[name]()
 
 
 if __name__ == "__main__":
