@@ -213,6 +213,9 @@ def main():
                                         outputs=STATE_KEYS[:16]),
         "rk2_c48_100.npz": lambda: gen_core(a.ref, a.out, "rk2_c48_100.npz", n=48, nbb=100, seed=7,
                                             keep_inputs=False, outputs=("h0", "ub", "vb")),
+        # the headline resolution (C96), RK2
+        "rk2_c96_10.npz": lambda: gen_core(a.ref, a.out, "rk2_c96_10.npz", n=96, nbb=10, seed=9,
+                                           keep_inputs=False, outputs=("h0", "ub", "vb")),
         # RK3 where tiles of the 8 x 16 and 16 x 16 shapes are full interior tiles
         "rk3_c48_30.npz": lambda: gen_core(a.ref, a.out, "rk3_c48_30.npz", n=48, nbb=30, seed=8, rk=3,
                                            keep_inputs=False, outputs=("h0", "ub", "vb")),

@@ -87,7 +87,8 @@ def test_stage_matches_reference(last, grids):
         assert_f64_close(a, z[f"{tag}_{name}"], f"{tag} {name}")
 
 
-CORES = ["rk2_c8.npz", "rk2_c12_base.npz", "rk3_c8.npz", "rk2_c24.npz", "rk2_c48_100.npz", "rk3_c48_30.npz"]
+CORES = ["rk2_c8.npz", "rk2_c12_base.npz", "rk3_c8.npz", "rk2_c24.npz", "rk2_c48_100.npz", "rk3_c48_30.npz",
+         "rk2_c96_10.npz"]
 
 
 @pytest.mark.parametrize("name", CORES)
@@ -347,18 +348,20 @@ def test_float32_full_tiles_c96(tile, grids):
 
 
 @pytest.mark.parametrize("full", [True, False])
-@pytest.mark.parametrize("tile", [(8, 16), (16, 16)])
-def test_rk3_c48_both_kernel_builds_match_reference(tile, full, grids):
-    """RK3, 30 substeps at C48 (full interior tiles at both shapes) against the reference's own
-    run, through the full-tile kernels and through the edge-path-only kernels."""
-    z = load_golden("rk3_c48_30.npz")
-    state, consts = golden_inputs(z, grids(48))
+@pytest.mark.parametrize("name,tile", [("rk3_c48_30.npz", (8, 16)), ("rk3_c48_30.npz", (16, 16)),
+                                       ("rk2_c96_10.npz", (8, 16)), ("rk2_c96_10.npz", (16, 32))])
+def test_both_kernel_builds_match_reference(name, tile, full, grids):
+    """RK3 at C48 and RK2 at C96 (the headline resolution), both with full interior tiles at these
+    shapes, against the reference's own runs, through the full-tile kernels and through the
+    edge-path-only kernels."""
+    z = load_golden(name)
+    state, consts = golden_inputs(z, grids(int(z["n"])))
     plan = BtPlan(consts, tile=tile, mode="graph")
     plan.set_full_tiles(full)
     six = [dev(s) for s in state[:6]]
-    out = plan.round(*six, nbb=int(z["nbb"]), dtb=float(z["dtb"]), rk=3, diag=False)
+    out = plan.round(*six, nbb=int(z["nbb"]), dtb=float(z["dtb"]), rk=int(z["rk"]), diag=False)
     for key in ("h0", "ub", "vb"):
-        assert_f64_close(out[key], z["out_" + key], f"rk3_c48_30 {tile} full={full}:{key}")
+        assert_f64_close(out[key], z["out_" + key], f"{name} {tile} full={full}:{key}")
     plan.close()
 
 

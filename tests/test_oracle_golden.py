@@ -14,7 +14,7 @@ from licom4py_gpu_b200.duogrid import make_consts
 from oracle import barotr_np as O
 
 CORE_FIXTURES = ["rk2_c8.npz", "rk2_c12_base.npz", "rk3_c8.npz", "rk2_c8_nbb0.npz", "rk2_c24.npz",
-                 "rk2_c48_100.npz", "rk3_c48_30.npz"]
+                 "rk2_c48_100.npz", "rk3_c48_30.npz", "rk2_c96_10.npz"]
 
 
 @pytest.mark.parametrize("name", CORE_FIXTURES + ["stage_c8.npz"])
