@@ -5,6 +5,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 
 #include "bt_batch.cuh"
 
@@ -277,8 +278,8 @@ size_t batch_round_smem() {
 // at once, recorded by prime_batch_tile (0 = not recorded).
 constexpr int kMaxBatchDevices = 64;
 template <typename T, int TI, int TJ, bool UV>
-int* batch_wave_slots() {
-  static int slots[kMaxBatchDevices] = {};
+std::atomic<int>* batch_wave_slots() {  // relaxed: plans on several host threads may record them at once
+  static std::atomic<int> slots[kMaxBatchDevices];
   return slots;
 }
 
@@ -296,7 +297,7 @@ cudaError_t prime_batch_phase() {
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_phase<T, TI, TJ, UV, false>, kTileThreads,
                                                          batch_tile_smem<T, TI, TJ, UV>())) != cudaSuccess)
     return e;
-  batch_wave_slots<T, TI, TJ, UV>()[dev] = sms * per_sm;
+  batch_wave_slots<T, TI, TJ, UV>()[dev].store(sms * per_sm, std::memory_order_relaxed);
   return cudaSuccess;
 }
 
@@ -345,7 +346,7 @@ cudaError_t launch_batch_phase_tile(const BatchArgs<T>& a, int step, int st, int
   cfg.numAttrs = 1;
   int dev = -1;
   const int slots = (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxBatchDevices)
-                        ? batch_wave_slots<T, TI, TJ, UV>()[dev] : 0;
+                        ? batch_wave_slots<T, TI, TJ, UV>()[dev].load(std::memory_order_relaxed) : 0;
   const bool one_wave = slots > 0 && ntiles <= slots;
   return one_wave ? cudaLaunchKernelEx(&cfg, k_batch_phase<T, TI, TJ, UV, false>, a, step, st, act)
                   : cudaLaunchKernelEx(&cfg, k_batch_phase<T, TI, TJ, UV, true>, a, step, st, act);

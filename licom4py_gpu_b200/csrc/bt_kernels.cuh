@@ -15,6 +15,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 
 #include "bt_launch.cuh"
 
@@ -228,8 +229,8 @@ size_t round_smem() {
 // recorded by prime_tile at plan creation (0 = not recorded yet).
 constexpr int kMaxDevices = 64;
 template <typename T, int TI, int TJ, bool UV>
-int* wave_slots() {
-  static int slots[kMaxDevices] = {};
+std::atomic<int>* wave_slots() {  // relaxed: plans on several host threads may record them at once
+  static std::atomic<int> slots[kMaxDevices];
   return slots;
 }
 
@@ -244,7 +245,7 @@ cudaError_t record_wave_slots() {
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, tile_smem<T, TI, TJ, UV>())) !=
       cudaSuccess)
     return e;
-  wave_slots<T, TI, TJ, UV>()[dev] = sms * per_sm;
+  wave_slots<T, TI, TJ, UV>()[dev].store(sms * per_sm, std::memory_order_relaxed);
   return cudaSuccess;
 }
 
@@ -294,7 +295,7 @@ bool full_path(int n, int full_tiles) {
   if (full_tiles >= 0) return full_tiles != 0;
   int dev = -1;
   const int slots =
-      (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) ? wave_slots<T, TI, TJ, UV>()[dev] : 0;
+      (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) ? wave_slots<T, TI, TJ, UV>()[dev].load(std::memory_order_relaxed) : 0;
   return !(slots > 0 && 6 * make_tiling({TI, TJ}, n).tiles_per_face() <= slots);
 }
 
