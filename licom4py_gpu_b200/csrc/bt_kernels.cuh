@@ -223,8 +223,6 @@ size_t round_smem() {
   return std::max(tile_smem<T, TI, TJ, false>(), tile_smem<T, TI, TJ, true>());
 }
 
-// Opt in to more than 48 KB of dynamic shared memory (done at plan creation,
-// never during stream capture).
 // CTAs of one phase kernel (edge-only build) that fit on each device at once,
 // recorded by prime_tile at plan creation (0 = not recorded yet).
 constexpr int kMaxDevices = 64;
@@ -249,6 +247,8 @@ cudaError_t record_wave_slots() {
   return cudaSuccess;
 }
 
+// Opt in to more than 48 KB of dynamic shared memory and record the wave slots
+// (done at plan creation, never during stream capture).
 template <typename T, int TI, int TJ>
 cudaError_t prime_tile() {
   cudaError_t e;
@@ -294,8 +294,9 @@ template <typename T, int TI, int TJ, bool UV>
 bool full_path(int n, int full_tiles) {
   if (full_tiles >= 0) return full_tiles != 0;
   int dev = -1;
-  const int slots =
-      (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) ? wave_slots<T, TI, TJ, UV>()[dev].load(std::memory_order_relaxed) : 0;
+  int slots = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices)
+    slots = wave_slots<T, TI, TJ, UV>()[dev].load(std::memory_order_relaxed);
   return !(slots > 0 && 6 * make_tiling({TI, TJ}, n).tiles_per_face() <= slots);
 }
 
